@@ -1,0 +1,262 @@
+// extern "C" entry points of libehss_b200.so (declared in include/ehss_b200.h).
+// Host-side validation mirrors the reference's ValueError checks; every
+// failure sets a thread-local message and returns a nonzero status.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include "ehss_internal.cuh"
+
+namespace ehss {
+
+static thread_local char g_error[512] = "";
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+}
+
+static const char* error_text() { return g_error; }
+static void clear_error() { g_error[0] = '\0'; }
+
+int cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return EHSS_OK;
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return EHSS_ERR_CUDA;
+}
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = n > 0 ? n : 148;
+    }
+    return cached[dev];
+}
+
+void sobol4_params(uint64_t seed, Sobol4Params* p) {
+    uint32_t sv[4 * 30], shift[4];
+    sobol_scramble(4, seed, sv, shift);
+    for (int k = 0; k < 30; ++k) p->sv[k] = make_uint4(sv[k], sv[30 + k], sv[60 + k], sv[90 + k]);
+    p->shift = make_uint4(shift[0], shift[1], shift[2], shift[3]);
+}
+
+}  // namespace ehss
+
+using namespace ehss;
+
+static cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+extern "C" {
+
+const char* ehss_last_error(void) { return error_text(); }
+
+int ehss_abi_version(void) { return EHSS_ABI_VERSION; }
+
+int ehss_sobol_scramble(int dim, uint64_t seed, uint32_t* sv_host, uint32_t* shift_host) {
+    clear_error();
+    if (!sv_host || !shift_host) { set_error("null output pointer"); return EHSS_ERR_VALUE; }
+    if (!sobol_scramble(dim, seed, sv_host, shift_host)) {
+        set_error("Sobol dimension must be 1..8, got %d", dim);
+        return EHSS_ERR_VALUE;
+    }
+    return EHSS_OK;
+}
+
+int ehss_sobol_points(int dim, uint64_t seed, int64_t first, int64_t n, uint32_t* q_dev, void* stream) {
+    clear_error();
+    if (dim < 1 || dim > 8) { set_error("Sobol dimension must be 1..8, got %d", dim); return EHSS_ERR_VALUE; }
+    if (first < 0 || n < 0 || first + n > (1ll << 30)) {
+        set_error("Sobol point range [%lld, %lld) outside 0..2^30", (long long)first, (long long)(first + n));
+        return EHSS_ERR_VALUE;
+    }
+    if (n > 0 && !q_dev) { set_error("null output pointer"); return EHSS_ERR_VALUE; }
+    SobolParams p;
+    memset(&p, 0, sizeof(p));
+    sobol_scramble(dim, seed, p.sv, p.shift);
+    return launch_sobol_points(dim, p, first, n, q_dev, as_stream(stream));
+}
+
+int ehss_scene_bytes(int64_t n_atoms, int leaf_size, uint64_t* scene_bytes, uint64_t* workspace_bytes) {
+    clear_error();
+    if (n_atoms < 1 || n_atoms > (1 << 27)) {
+        set_error("atom count %lld outside 1..2^27", (long long)n_atoms);
+        return EHSS_ERR_VALUE;
+    }
+    if (leaf_size < 1 || leaf_size > kMaxLeaf) { set_error("leaf_size must be 1..%d", kMaxLeaf); return EHSS_ERR_VALUE; }
+    uint64_t a, b, c, d, e, total;
+    scene_layout(n_atoms, &a, &b, &c, &d, &e, &total);
+    if (scene_bytes) *scene_bytes = total;
+    if (workspace_bytes) *workspace_bytes = build_workspace_bytes(n_atoms, 1);
+    return EHSS_OK;
+}
+
+int ehss_scene_build(int64_t n_atoms, const double* xyz_dev, const double* radii_dev, int leaf_size, void* scene_dev,
+                     uint64_t scene_bytes, void* workspace_dev, uint64_t workspace_bytes, void* stream) {
+    clear_error();
+    if (!xyz_dev || !radii_dev || !scene_dev || !workspace_dev) { set_error("null pointer"); return EHSS_ERR_VALUE; }
+    return build_scenes(1, &xyz_dev, &radii_dev, &n_atoms, leaf_size, &scene_dev, &scene_bytes, workspace_dev,
+                        workspace_bytes, as_stream(stream));
+}
+
+int ehss_scenes_workspace_bytes(int n_scenes, const int64_t* n_atoms_host, uint64_t* workspace_bytes) {
+    clear_error();
+    if (n_scenes < 1 || !n_atoms_host || !workspace_bytes) { set_error("invalid arguments"); return EHSS_ERR_VALUE; }
+    int64_t N = 0;
+    for (int s = 0; s < n_scenes; ++s) {
+        if (n_atoms_host[s] < 1) { set_error("structure %d has no atoms", s); return EHSS_ERR_VALUE; }
+        N += n_atoms_host[s];
+    }
+    *workspace_bytes = build_workspace_bytes(N, n_scenes);
+    return EHSS_OK;
+}
+
+int ehss_scenes_build(int n_scenes, const double* const* xyz_dev, const double* const* radii_dev,
+                      const int64_t* n_atoms_host, int leaf_size, void* const* scenes_dev,
+                      const uint64_t* scene_bytes_host, void* workspace_dev, uint64_t workspace_bytes, void* stream) {
+    clear_error();
+    if (n_scenes < 1 || !xyz_dev || !radii_dev || !n_atoms_host || !scenes_dev || !scene_bytes_host ||
+        !workspace_dev) {
+        set_error("invalid arguments");
+        return EHSS_ERR_VALUE;
+    }
+    return build_scenes(n_scenes, xyz_dev, radii_dev, n_atoms_host, leaf_size, scenes_dev, scene_bytes_host,
+                        workspace_dev, workspace_bytes, as_stream(stream));
+}
+
+int ehss_scene_info_get(const void* scene_dev, ehss_scene_info* info, void* stream) {
+    clear_error();
+    if (!scene_dev || !info) { set_error("null pointer"); return EHSS_ERR_VALUE; }
+    SceneHeader h;
+    int rc = cuda_status(cudaMemcpyAsync(&h, scene_dev, sizeof(h), cudaMemcpyDeviceToHost, as_stream(stream)),
+                         "scene header read");
+    if (rc) return rc;
+    rc = cuda_status(cudaStreamSynchronize(as_stream(stream)), "scene header read");
+    if (rc) return rc;
+    if (h.magic != kSceneMagic) { set_error("not a built scene buffer"); return EHSS_ERR_VALUE; }
+    if (h.status != 0) { set_error("scene input has a non-positive or non-finite radius or coordinate"); return EHSS_ERR_VALUE; }
+    info->n_atoms = h.n_atoms;
+    info->n_nodes = h.n_nodes;
+    info->leaf_size = h.leaf_size;
+    info->depth = h.depth;
+    for (int c = 0; c < 3; ++c) info->center[c] = h.center[c];
+    info->radius = h.radius;
+    info->scale = h.scale;
+    info->rmax = h.rmax;
+    info->bytes = h.bytes;
+    return EHSS_OK;
+}
+
+int ehss_source_rays(const void* scene_dev, int log2n, uint64_t seed, int64_t first, int64_t n, double* origins_dev,
+                     double* directions_dev, void* stream) {
+    clear_error();
+    if (!scene_dev) { set_error("null scene"); return EHSS_ERR_VALUE; }
+    if (log2n < 0 || log2n > 30) { set_error("log2n must be 0..30"); return EHSS_ERR_VALUE; }
+    if (first < 0 || n < 0 || first + n > (1ll << log2n)) { set_error("ray range outside the sequence"); return EHSS_ERR_VALUE; }
+    if (n > 0 && (!origins_dev || !directions_dev)) { set_error("null output pointer"); return EHSS_ERR_VALUE; }
+    Sobol4Params p;
+    sobol4_params(seed, &p);
+    return launch_source_rays(scene_dev, p, first, n, origins_dev, directions_dev, as_stream(stream));
+}
+
+int ehss_trace(const void* scene_dev, int64_t n_rays, int cap, int precision, double* positions_dev,
+               double* directions_dev, const int64_t* last_atom_dev, int64_t* bounces_dev, uint8_t* escaped_dev,
+               uint8_t* unresolved_dev, int32_t* history_dev, uint64_t* stats_dev, void* stream) {
+    clear_error();
+    if (cap < 1) { set_error("Positive cap and zero/one initial collision required"); return EHSS_ERR_VALUE; }
+    if (precision != EHSS_PREC_FP64 && precision != EHSS_PREC_FP32) { set_error("unknown precision %d", precision); return EHSS_ERR_VALUE; }
+    if (n_rays < 0) { set_error("negative ray count"); return EHSS_ERR_VALUE; }
+    if (n_rays > 0 && (!scene_dev || !positions_dev || !directions_dev || !last_atom_dev || !bounces_dev ||
+                       !escaped_dev || !unresolved_dev)) {
+        set_error("null pointer");
+        return EHSS_ERR_VALUE;
+    }
+    return launch_trace_rays(scene_dev, n_rays, cap, precision, positions_dev, directions_dev, last_atom_dev,
+                             bounces_dev, escaped_dev, unresolved_dev, history_dev, stats_dev, as_stream(stream));
+}
+
+int ehss_pa_anyhit(const void* scene_dev, int64_t n_rays, const double* origins_dev, const double* directions_dev,
+                   const int64_t* owners_dev, uint8_t* blocked_dev, uint64_t* stats_dev, void* stream) {
+    clear_error();
+    if (n_rays < 0) { set_error("negative ray count"); return EHSS_ERR_VALUE; }
+    if (n_rays > 0 && (!scene_dev || !origins_dev || !directions_dev || !blocked_dev)) {
+        set_error("null pointer");
+        return EHSS_ERR_VALUE;
+    }
+    return launch_pa_rays(scene_dev, n_rays, origins_dev, directions_dev, owners_dev, blocked_dev, stats_dev,
+                          as_stream(stream));
+}
+
+int ehss_blocks_prepare(ehss_block* blocks, int n_blocks, const uint64_t* seeds, int chunk_rays, int64_t* total_chunks) {
+    clear_error();
+    if (!blocks || !seeds || !total_chunks || n_blocks < 1) { set_error("invalid arguments"); return EHSS_ERR_VALUE; }
+    if (chunk_rays < 32 || chunk_rays > 4096 || (chunk_rays & (chunk_rays - 1))) {
+        set_error("chunk_rays must be a power of two in 32..4096");
+        return EHSS_ERR_VALUE;
+    }
+    int64_t total = 0, hist = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+        ehss_block& B = blocks[b];
+        if (!B.scene) { set_error("block %d: null scene", b); return EHSS_ERR_VALUE; }
+        if (B.log2_rays < 3 || B.log2_rays > 24) { set_error("block %d: log2_rays must be 3..24", b); return EHSS_ERR_VALUE; }
+        if (B.cap < 1 || B.cap > 100000) { set_error("block %d: cap must be 1..100000", b); return EHSS_ERR_VALUE; }
+        if (B.precision != EHSS_PREC_FP64 && B.precision != EHSS_PREC_FP32) { set_error("block %d: unknown precision", b); return EHSS_ERR_VALUE; }
+        if (!(B.flags & (EHSS_BLOCK_EHSS | EHSS_BLOCK_PA))) { set_error("block %d: no work flags", b); return EHSS_ERR_VALUE; }
+        if (B.hist_offset < 0) B.hist_offset = hist;
+        hist = B.hist_offset + B.cap + 1;
+        Sobol4Params p;
+        sobol4_params(seeds[b], &p);
+        for (int k = 0; k < 30; ++k) {
+            B.sv[k][0] = p.sv[k].x; B.sv[k][1] = p.sv[k].y; B.sv[k][2] = p.sv[k].z; B.sv[k][3] = p.sv[k].w;
+        }
+        B.shift[0] = p.shift.x; B.shift[1] = p.shift.y; B.shift[2] = p.shift.z; B.shift[3] = p.shift.w;
+        B.chunk_begin = total;
+        int64_t n = 1ll << B.log2_rays;
+        total += (n + chunk_rays - 1) / chunk_rays;
+    }
+    *total_chunks = total;
+    return EHSS_OK;
+}
+
+int ehss_blocks_workspace_bytes(int n_blocks, uint64_t* bytes) {
+    clear_error();
+    if (n_blocks < 1 || !bytes) { set_error("invalid arguments"); return EHSS_ERR_VALUE; }
+    *bytes = 256;
+    return EHSS_OK;
+}
+
+int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks, ehss_block_result* results_dev,
+                      uint64_t* hist_dev, uint64_t* ledger_dev, int64_t hist_entries, void* workspace_dev,
+                      uint64_t workspace_bytes, const ehss_launch* launch, void* stream) {
+    clear_error();
+    if (!blocks_dev || n_blocks < 1 || !results_dev || !hist_dev || !ledger_dev || !workspace_dev || !launch) {
+        set_error("invalid arguments");
+        return EHSS_ERR_VALUE;
+    }
+    if (workspace_bytes < 256) { set_error("blocks workspace must hold 256 bytes"); return EHSS_ERR_CAPACITY; }
+    const ehss_launch& L = *launch;
+    if (L.block_threads < 64 || L.block_threads > 256 || L.block_threads % 32) {
+        set_error("block_threads must be a multiple of 32 in 64..256");
+        return EHSS_ERR_VALUE;
+    }
+    if (L.ctas_per_sm < 1 || L.ctas_per_sm > 32) { set_error("ctas_per_sm must be 1..32"); return EHSS_ERR_VALUE; }
+    if (L.chunk_rays < 32 || L.chunk_rays > 4096 || (L.chunk_rays & (L.chunk_rays - 1))) {
+        set_error("chunk_rays must be a power of two in 32..4096");
+        return EHSS_ERR_VALUE;
+    }
+    cudaStream_t s = as_stream(stream);
+    int rc = cuda_status(cudaMemsetAsync(results_dev, 0, sizeof(ehss_block_result) * (size_t)n_blocks, s), "result reset");
+    if (!rc && hist_entries > 0) rc = cuda_status(cudaMemsetAsync(hist_dev, 0, 8ull * hist_entries, s), "hist reset");
+    if (!rc && hist_entries > 0) rc = cuda_status(cudaMemsetAsync(ledger_dev, 0, 8ull * hist_entries, s), "ledger reset");
+    if (!rc) rc = cuda_status(cudaMemsetAsync(workspace_dev, 0, 8, s), "work counter reset");
+    if (rc) return rc;
+    if (total_chunks == 0) return EHSS_OK;
+    return launch_blocks(blocks_dev, n_blocks, total_chunks, L, results_dev, hist_dev, ledger_dev,
+                         reinterpret_cast<unsigned long long*>(workspace_dev), s);
+}
+
+}  // extern "C"

@@ -1,0 +1,514 @@
+// Device LBVH scene builder (batched over structures).
+//
+// Replaces the reference's static preparation (PreparedStaticCPUEHSS,
+// src/support_exchange_transport/ehss_static.py:62-101: median groups,
+// implicit topology, padded leaf bounds, parent unions) and the PA index
+// build (SphereIndex / build_tree, pa_spatial.py:38-75, 157-160).  The tree
+// differs by design -- results do not depend on it, because every traversal
+// keeps the reference's (distance, atom id) minimum and prunes only boxes
+// that provably contain no nearer entry.
+//
+// Pipeline (one launch each, all structures of a batch at once):
+//   1. k_stats     per structure: sequential FP64 mean of the centres (the
+//                  order numpy's mean(axis=0) uses), enclosing radius R,
+//                  scale S, largest radius, centre bounds, input validation
+//   2. k_morton    per atom: 30-bit Morton code of the centre in its
+//                  structure's centre box; key = structure << 30 | code
+//   3. CUB radix sort of (key, atom) pairs -- stable, so equal codes keep
+//                  atom order
+//   4. k_karras    per internal node: Karras (2012) range / split search
+//                  within the structure's segment
+//   5. k_refit     per atom: FP32 boxes rounded outward, unioned bottom-up
+//                  with one atomic arrival counter per internal node
+//   6. k_emit      per internal node: 64-byte traversal record with both
+//                  child boxes (expanded by eps_box), subtrees of at most
+//                  leaf_size atoms collapsed into leaf references; per atom:
+//                  FP32 and FP64 atom records in leaf order, id maps.
+#include <cub/device/device_radix_sort.cuh>
+#include <cstdio>
+#include <cstring>
+#include "ehss_internal.cuh"
+
+namespace ehss {
+
+struct BuildDesc {
+    const double* xyz;
+    const double* radii;
+    char* scene;
+    int64_t n;
+    int64_t atom0;       // first global atom index
+    int64_t inner0;      // first global internal-node index
+    int32_t leaf_size;
+    int32_t pad;
+    double cmin[3], cext[3];   // centre box relative to the scene centre (filled by k_stats)
+};
+
+struct BuildWork {
+    BuildDesc* descs;
+    int32_t* atom_scene;     // [N] structure of each global atom
+    uint64_t* keys_in;       // [N]
+    uint64_t* keys_out;      // [N]
+    int32_t* vals_in;        // [N]
+    int32_t* vals_out;       // [N]
+    int32_t* inner_child;    // [2*I] child refs of Karras internal nodes (>=0 inner local idx, <0 ~leaf)
+    int32_t* inner_range;    // [2*I] first/last sorted position (local)
+    int32_t* parent_inner;   // [I]   parent local inner index of each internal node (-1 root)
+    int32_t* parent_leaf;    // [N]   parent local inner index of each leaf
+    float* inner_box;        // [6*I]
+    float* leaf_box;         // [6*N]
+    int32_t* inner_height;   // [I]
+    uint32_t* arrivals;      // [I]
+    void* cub_temp;
+    size_t cub_bytes;
+};
+
+// --------------------------------------------------------------------------
+__global__ void k_stats(BuildDesc* descs, int n_scenes) {
+    int s = blockIdx.x;
+    if (s >= n_scenes) return;
+    BuildDesc& D = descs[s];
+    SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
+    const int64_t n = D.n;
+    __shared__ double center[3];
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    // Sequential sum, one lane per coordinate: numpy's mean(axis=0) adds the
+    // rows in order and divides by n (ehss_state.py:46).
+    if (threadIdx.x < 3) {
+        int c = threadIdx.x;
+        double acc = 0.;
+        for (int64_t i = 0; i < n; ++i) acc = dadd(acc, D.xyz[i * 3 + c]);
+        center[c] = ddiv(acc, (double)n);
+    }
+    // validation and radii extrema
+    double rmax = 0.;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        double r = D.radii[i];
+        double x = D.xyz[i * 3], y = D.xyz[i * 3 + 1], z = D.xyz[i * 3 + 2];
+        if (!(r > 0.) || !isfinite(r) || !isfinite(x) || !isfinite(y) || !isfinite(z)) bad = 1;
+        rmax = fmax(rmax, r);
+    }
+    __syncthreads();
+    // R = max(|c_j - center| + r_j) * (1 + 1e-9) (ehss_state.py:47); norm as
+    // numpy's linalg.norm(axis=1): sqrt((x*x + y*y) + z*z).
+    double smax = 0.;
+    double lo[3] = {CUDART_INF, CUDART_INF, CUDART_INF}, hi[3] = {-CUDART_INF, -CUDART_INF, -CUDART_INF};
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        double x = dsub(D.xyz[i * 3], center[0]);
+        double y = dsub(D.xyz[i * 3 + 1], center[1]);
+        double z = dsub(D.xyz[i * 3 + 2], center[2]);
+        double len = dadd(dsqrt(dadd(dadd(dmul(x, x), dmul(y, y)), dmul(z, z))), D.radii[i]);
+        smax = fmax(smax, len);
+        lo[0] = fmin(lo[0], x); lo[1] = fmin(lo[1], y); lo[2] = fmin(lo[2], z);
+        hi[0] = fmax(hi[0], x); hi[1] = fmax(hi[1], y); hi[2] = fmax(hi[2], z);
+    }
+    // block-wide maxima (order-independent): warp shuffles, then one warp
+    __shared__ double partial[8][32];
+    __shared__ double result[8];
+    double vals[8] = {rmax, smax, -lo[0], -lo[1], -lo[2], hi[0], hi[1], hi[2]};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int k = 0; k < 8; ++k) {
+        double m = vals[k];
+        for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+        if (lane == 0) partial[k][warp] = m;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int k = 0; k < 8; ++k) {
+            double m = lane < nwarps ? partial[k][lane] : -CUDART_INF;
+            for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+            if (lane == 0) result[k] = m;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        H->magic = kSceneMagic;
+        H->status = bad ? 1 : 0;
+        H->n_atoms = (int32_t)n;
+        H->leaf_size = D.leaf_size;
+        for (int c = 0; c < 3; ++c) H->center[c] = center[c];
+        H->rmax = result[0];
+        H->scale = result[1];
+        H->radius = dmul(result[1], 1.000000001);
+        H->scale_f = __double2float_ru(result[1]);
+        H->rmax_f = __double2float_ru(result[0]);
+        // FP32 box expansion: 2^-14 S covers the FP32 rounding of any ray
+        // whose origin lies within 3 S of the centre (the traversal sends
+        // farther origins to the FP64 all-atom search).
+        H->eps_box = __double2float_ru(result[1] * 0x1p-14);
+        for (int c = 0; c < 3; ++c) {
+            D.cmin[c] = -result[2 + c];
+            D.cext[c] = result[5 + c] + result[2 + c];
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__global__ void k_morton(const BuildDesc* descs, const int32_t* atom_scene, int64_t N, uint64_t* keys, int32_t* vals) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= N) return;
+    int s = atom_scene[g];
+    const BuildDesc& D = descs[s];
+    const SceneHeader* H = reinterpret_cast<const SceneHeader*>(D.scene);
+    int64_t i = g - D.atom0;
+    uint32_t q[3];
+    for (int c = 0; c < 3; ++c) {
+        double rel = (D.xyz[i * 3 + c] - H->center[c]) - D.cmin[c];
+        double e = D.cext[c];
+        double u = e > 0. ? rel / e : 0.;
+        u = fmin(fmax(u, 0.), 1.);
+        q[c] = (uint32_t)fmin(u * 1024.0, 1023.0);
+    }
+    uint32_t code = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+    keys[g] = ((uint64_t)s << 30) | code;
+    vals[g] = (int32_t)i;
+}
+
+// Karras (2012), "Maximizing parallelism in the construction of BVHs,
+// octrees, and k-d trees": internal node i of a segment of n sorted keys.
+__device__ __forceinline__ int delta(const uint64_t* k, int64_t base, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint64_t a = k[base + i], b = k[base + j];
+    if (a == b) return 64 + __clz((uint32_t)(i ^ j));
+    return __clzll(a ^ b);
+}
+
+__global__ void k_karras(const BuildDesc* descs, int n_scenes, int64_t I_total, const uint64_t* keys,
+                         int32_t* inner_child, int32_t* inner_range, int32_t* parent_inner, int32_t* parent_leaf) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= I_total) return;
+    // structure owning inner node g: last s with inner0 <= g (binary search)
+    int lo = 0, hi = n_scenes - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].inner0 <= g) lo = mid; else hi = mid - 1;
+    }
+    const BuildDesc& D = descs[lo];
+    int n = (int)D.n;
+    int i = (int)(g - D.inner0);
+    if (i >= n - 1) return;   // structures with one atom own no internal node
+    int64_t base = D.atom0;
+    int d = (delta(keys, base, n, i, i + 1) - delta(keys, base, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(keys, base, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, base, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, base, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta(keys, base, n, i, j);
+    int s = 0;
+    int span = l;
+    for (int t = (span + 1) >> 1;; t = (t + 1) >> 1) {
+        if (delta(keys, base, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t == 1) break;
+    }
+    int gamma = i + s * d + (d < 0 ? d : 0);
+    int first = i < j ? i : j, last = i < j ? j : i;
+    int64_t gi = D.inner0 + i;
+    inner_range[2 * gi] = first;
+    inner_range[2 * gi + 1] = last;
+    int left = (first == gamma) ? ~gamma : gamma;
+    int right = (last == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    inner_child[2 * gi] = left;
+    inner_child[2 * gi + 1] = right;
+    if (left < 0) parent_leaf[base + gamma] = i; else parent_inner[D.inner0 + left] = i;
+    if (right < 0) parent_leaf[base + gamma + 1] = i; else parent_inner[D.inner0 + right] = i;
+    if (i == 0) parent_inner[gi] = -1;
+}
+
+__device__ __forceinline__ void atom_box(const BuildDesc& D, const SceneHeader* H, int64_t atom, float* b) {
+    double r = D.radii[atom];
+    for (int c = 0; c < 3; ++c) {
+        double rel = D.xyz[atom * 3 + c] - H->center[c];
+        b[c] = __double2float_rd(rel - r);
+        b[3 + c] = __double2float_ru(rel + r);
+    }
+}
+
+__global__ void k_refit(const BuildDesc* descs, const int32_t* atom_scene, int64_t N, const int32_t* vals_sorted,
+                        const int32_t* inner_child, const int32_t* parent_inner, const int32_t* parent_leaf,
+                        float* inner_box, float* leaf_box, int32_t* inner_height, uint32_t* arrivals) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= N) return;
+    const BuildDesc& D = descs[atom_scene[g]];
+    const SceneHeader* H = reinterpret_cast<const SceneHeader*>(D.scene);
+    float b[6];
+    atom_box(D, H, vals_sorted[g], b);
+    for (int k = 0; k < 6; ++k) leaf_box[6 * g + k] = b[k];
+    if (D.n == 1) return;
+    int node = parent_leaf[g];
+    __threadfence();
+    // a walk longer than any LBVH depth (Morton bits + duplicate bits) means a malformed link
+    for (int hops = 0; node >= 0 && node < D.n - 1 && hops < 128; ++hops) {
+        int64_t gi = D.inner0 + node;
+        if (atomicAdd(&arrivals[gi], 1u) == 0) return;   // the sibling subtree is not finished yet
+        __threadfence();
+        float u[6] = {CUDART_INF_F, CUDART_INF_F, CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F};
+        int h = 0;
+        for (int side = 0; side < 2; ++side) {
+            int c = inner_child[2 * gi + side];
+            const float* src;
+            int hc;
+            if (c < 0 ? (~c >= D.n) : (c >= D.n - 1)) return;   // malformed link: leave the node unset
+            if (c < 0) { src = leaf_box + 6 * (D.atom0 + ~c); hc = 0; }
+            else { src = inner_box + 6 * (D.inner0 + c); hc = __ldcg(inner_height + D.inner0 + c); }
+            for (int k = 0; k < 3; ++k) {
+                u[k] = fminf(u[k], __ldcg(src + k));
+                u[3 + k] = fmaxf(u[3 + k], __ldcg(src + 3 + k));
+            }
+            h = max(h, hc);
+        }
+        for (int k = 0; k < 6; ++k) inner_box[6 * gi + k] = u[k];
+        inner_height[gi] = h + 1;
+        __threadfence();
+        node = parent_inner[gi];
+    }
+}
+
+__device__ __forceinline__ void put_child_box(float4& nxy, float& lz, float& hz, const float* b, float eps) {
+    nxy = make_float4(__fsub_rd(b[0], eps), __fadd_ru(b[3], eps), __fsub_rd(b[1], eps), __fadd_ru(b[4], eps));
+    lz = __fsub_rd(b[2], eps);
+    hz = __fadd_ru(b[5], eps);
+}
+
+__global__ void k_emit_nodes(const BuildDesc* descs, int n_scenes, int64_t I_total, const int32_t* inner_child,
+                             const int32_t* inner_range, const float* inner_box, const float* leaf_box,
+                             const int32_t* inner_height) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    // one extra thread per structure handles the single-leaf case (n <= leaf_size)
+    if (g >= I_total + n_scenes) return;
+    if (g >= I_total) {
+        const BuildDesc& D = descs[g - I_total];
+        SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
+        if (D.n > D.leaf_size) {
+            H->depth = inner_height[D.inner0];
+            H->n_nodes = (int32_t)(D.n - 1);
+            return;
+        }
+        // whole structure in one leaf below a single node
+        float4* nodes = reinterpret_cast<float4*>(D.scene + H->off_nodes);
+        float u[6] = {CUDART_INF_F, CUDART_INF_F, CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F};
+        for (int64_t a = 0; a < D.n; ++a)
+            for (int k = 0; k < 3; ++k) {
+                u[k] = fminf(u[k], leaf_box[6 * (D.atom0 + a) + k]);
+                u[3 + k] = fmaxf(u[3 + k], leaf_box[6 * (D.atom0 + a) + 3 + k]);
+            }
+        float4 n0; float lz, hz;
+        put_child_box(n0, lz, hz, u, H->eps_box);
+        nodes[0] = n0;
+        nodes[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        nodes[2] = make_float4(lz, hz, 0.f, 0.f);
+        int leaf = ~((0 << 3) | (int)(D.n - 1));
+        nodes[3] = make_float4(__int_as_float(leaf), __int_as_float(INT32_MIN), 0.f, 0.f);
+        H->depth = 1;
+        H->n_nodes = 1;
+        return;
+    }
+    int lo = 0, hi = n_scenes - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].inner0 <= g) lo = mid; else hi = mid - 1;
+    }
+    const BuildDesc& D = descs[lo];
+    int i = (int)(g - D.inner0);
+    if (i >= D.n - 1 || D.n <= D.leaf_size) return;
+    SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
+    float4* nodes = reinterpret_cast<float4*>(D.scene + H->off_nodes) + 4 * (int64_t)i;
+    float eps = H->eps_box;
+    int refs[2];
+    float4 nxy[2];
+    float lz[2], hz[2];
+    for (int side = 0; side < 2; ++side) {
+        int c = inner_child[2 * g + side];
+        const float* box;
+        if (c < 0) {
+            box = leaf_box + 6 * (D.atom0 + ~c);
+            refs[side] = ~((~c) << 3);                    // one atom
+        } else {
+            box = inner_box + 6 * (D.inner0 + c);
+            int first = inner_range[2 * (D.inner0 + c)], last = inner_range[2 * (D.inner0 + c) + 1];
+            int count = last - first + 1;
+            refs[side] = (count <= D.leaf_size) ? ~((first << 3) | (count - 1)) : c;
+        }
+        put_child_box(nxy[side], lz[side], hz[side], box, eps);
+    }
+    nodes[0] = nxy[0];
+    nodes[1] = nxy[1];
+    nodes[2] = make_float4(lz[0], hz[0], lz[1], hz[1]);
+    nodes[3] = make_float4(__int_as_float(refs[0]), __int_as_float(refs[1]), 0.f, 0.f);
+}
+
+__global__ void k_emit_atoms(const BuildDesc* descs, const int32_t* atom_scene, int64_t N, const int32_t* vals_sorted) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= N) return;
+    const BuildDesc& D = descs[atom_scene[g]];
+    SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
+    int64_t j = g - D.atom0;               // leaf-order position
+    int64_t a = vals_sorted[g];            // input atom id
+    float4* atoms = reinterpret_cast<float4*>(D.scene + H->off_atoms);
+    double4* atoms64 = reinterpret_cast<double4*>(D.scene + H->off_atoms64);
+    int32_t* ids = reinterpret_cast<int32_t*>(D.scene + H->off_ids);
+    int32_t* rank = reinterpret_cast<int32_t*>(D.scene + H->off_rank);
+    double x = D.xyz[a * 3], y = D.xyz[a * 3 + 1], z = D.xyz[a * 3 + 2], r = D.radii[a];
+    atoms[j] = make_float4(__double2float_rn(x - H->center[0]), __double2float_rn(y - H->center[1]),
+                           __double2float_rn(z - H->center[2]), __double2float_rn(r));
+    atoms64[j] = make_double4(x, y, z, r);
+    ids[j] = (int32_t)a;
+    rank[a] = (int32_t)j;
+}
+
+__global__ void k_fill_scene_index(const BuildDesc* descs, int n_scenes, int32_t* atom_scene) {
+    int s = blockIdx.x;
+    if (s >= n_scenes) return;
+    const BuildDesc& D = descs[s];
+    for (int64_t i = threadIdx.x; i < D.n; i += blockDim.x) atom_scene[D.atom0 + i] = s;
+}
+
+// --------------------------------------------------------------------------
+// Host side
+// --------------------------------------------------------------------------
+static size_t cub_sort_bytes(int64_t N) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint64_t*)nullptr, (uint64_t*)nullptr,
+                                    (const int32_t*)nullptr, (int32_t*)nullptr, (int)(N > 0 ? N : 1));
+    return bytes;
+}
+
+// Workspace for a batch with N atoms over S structures.
+uint64_t build_workspace_bytes(int64_t N, int S) {
+    int64_t I = N > 0 ? N : 1;
+    uint64_t b = 0;
+    b += align256(sizeof(BuildDesc) * (uint64_t)S);
+    b += align256(4ull * N);            // atom_scene
+    b += 2 * align256(8ull * N);        // keys
+    b += 2 * align256(4ull * N);        // vals
+    b += align256(8ull * I);            // inner_child
+    b += align256(8ull * I);            // inner_range
+    b += align256(4ull * I);            // parent_inner
+    b += align256(4ull * N);            // parent_leaf
+    b += align256(24ull * I);           // inner_box
+    b += align256(24ull * N);           // leaf_box
+    b += align256(4ull * I);            // inner_height
+    b += align256(4ull * I);            // arrivals
+    b += align256(cub_sort_bytes(N));
+    return b + 256;
+}
+
+int build_scenes(int S, const double* const* xyz, const double* const* radii, const int64_t* n, int leaf_size,
+                 void* const* scenes, const uint64_t* scene_bytes, void* workspace, uint64_t workspace_bytes,
+                 cudaStream_t stream) {
+    if (S < 1) { set_error("at least one structure required"); return EHSS_ERR_VALUE; }
+    if (leaf_size < 1 || leaf_size > kMaxLeaf) { set_error("leaf_size must be 1..%d", kMaxLeaf); return EHSS_ERR_VALUE; }
+    int64_t N = 0, I = 0;
+    BuildDesc* host = new BuildDesc[S];
+    for (int s = 0; s < S; ++s) {
+        if (n[s] < 1 || n[s] > (1 << 27)) {
+            delete[] host;
+            set_error("structure %d: atom count %lld outside 1..2^27", s, (long long)n[s]);
+            return EHSS_ERR_VALUE;
+        }
+        uint64_t on, oa, o64, oi, orr, total;
+        scene_layout(n[s], &on, &oa, &o64, &oi, &orr, &total);
+        if (scene_bytes[s] < total) {
+            delete[] host;
+            set_error("structure %d: scene buffer holds %llu bytes, %llu required", s,
+                      (unsigned long long)scene_bytes[s], (unsigned long long)total);
+            return EHSS_ERR_CAPACITY;
+        }
+        if (((uintptr_t)scenes[s] & 255u) != 0) {
+            delete[] host;
+            set_error("structure %d: scene buffer must be 256-byte aligned", s);
+            return EHSS_ERR_VALUE;
+        }
+        BuildDesc& D = host[s];
+        D.xyz = xyz[s]; D.radii = radii[s]; D.scene = (char*)scenes[s];
+        D.n = n[s]; D.atom0 = N; D.inner0 = I; D.leaf_size = leaf_size; D.pad = 0;
+        N += n[s];
+        I += n[s] - 1;
+    }
+    uint64_t need = build_workspace_bytes(N, S);
+    if (workspace_bytes < need) {
+        delete[] host;
+        set_error("build workspace holds %llu bytes, %llu required", (unsigned long long)workspace_bytes,
+                  (unsigned long long)need);
+        return EHSS_ERR_CAPACITY;
+    }
+    char* p = (char*)(((uintptr_t)workspace + 255u) & ~(uintptr_t)255u);
+    BuildWork W;
+    int64_t Ia = I > 0 ? I : 1;
+    W.descs = (BuildDesc*)p; p += align256(sizeof(BuildDesc) * (uint64_t)S);
+    W.atom_scene = (int32_t*)p; p += align256(4ull * N);
+    W.keys_in = (uint64_t*)p; p += align256(8ull * N);
+    W.keys_out = (uint64_t*)p; p += align256(8ull * N);
+    W.vals_in = (int32_t*)p; p += align256(4ull * N);
+    W.vals_out = (int32_t*)p; p += align256(4ull * N);
+    W.inner_child = (int32_t*)p; p += align256(8ull * Ia);
+    W.inner_range = (int32_t*)p; p += align256(8ull * Ia);
+    W.parent_inner = (int32_t*)p; p += align256(4ull * Ia);
+    W.parent_leaf = (int32_t*)p; p += align256(4ull * N);
+    W.inner_box = (float*)p; p += align256(24ull * Ia);
+    W.leaf_box = (float*)p; p += align256(24ull * N);
+    W.inner_height = (int32_t*)p; p += align256(4ull * Ia);
+    W.arrivals = (uint32_t*)p; p += align256(4ull * Ia);
+    W.cub_temp = p;
+    W.cub_bytes = cub_sort_bytes(N);
+
+    // headers: layout offsets are host-computed, the rest is filled on device
+    for (int s = 0; s < S; ++s) {
+        SceneHeader h;
+        memset(&h, 0, sizeof(h));
+        uint64_t total;
+        scene_layout(n[s], &h.off_nodes, &h.off_atoms, &h.off_atoms64, &h.off_ids, &h.off_rank, &total);
+        h.bytes = total;
+        int rc = cuda_status(cudaMemcpyAsync(scenes[s], &h, sizeof(h), cudaMemcpyHostToDevice, stream),
+                             "scene header upload");
+        if (rc) { delete[] host; return rc; }
+    }
+    int rc = cuda_status(cudaMemcpyAsync(W.descs, host, sizeof(BuildDesc) * S, cudaMemcpyHostToDevice, stream),
+                         "build descriptor upload");
+    if (rc) { delete[] host; return rc; }
+    // pageable copies above are staged before returning, so the host array may go
+    rc = cuda_status(cudaStreamSynchronize(stream), "build descriptor upload");
+    delete[] host;
+    if (rc) return rc;
+
+    const int T = 256;
+    auto blocks = [&](int64_t count) { return (unsigned)((count + T - 1) / T); };
+    k_fill_scene_index<<<S, 256, 0, stream>>>(W.descs, S, W.atom_scene);
+    k_stats<<<S, 256, 0, stream>>>(W.descs, S);
+    k_morton<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, W.keys_in, W.vals_in);
+    int end_bit = 30;
+    while ((1ll << (end_bit - 30)) < S) ++end_bit;
+    size_t cub_bytes = W.cub_bytes;
+    rc = cuda_status(cub::DeviceRadixSort::SortPairs(W.cub_temp, cub_bytes, W.keys_in, W.keys_out, W.vals_in,
+                                                     W.vals_out, (int)N, 0, end_bit, stream), "LBVH key sort");
+    if (rc) return rc;
+    // parent links start at -1 so that a missing link ends a refit walk
+    rc = cuda_status(cudaMemsetAsync(W.parent_leaf, 0xff, 4ull * N, stream), "LBVH parent reset");
+    if (rc) return rc;
+    if (I > 0) {
+        rc = cuda_status(cudaMemsetAsync(W.arrivals, 0, 4ull * I, stream), "LBVH arrival reset");
+        if (!rc) rc = cuda_status(cudaMemsetAsync(W.parent_inner, 0xff, 4ull * I, stream), "LBVH parent reset");
+        if (rc) return rc;
+        k_karras<<<blocks(I), T, 0, stream>>>(W.descs, S, I, W.keys_out, W.inner_child, W.inner_range,
+                                              W.parent_inner, W.parent_leaf);
+    }
+    k_refit<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, W.vals_out, W.inner_child, W.parent_inner,
+                                         W.parent_leaf, W.inner_box, W.leaf_box, W.inner_height, W.arrivals);
+    k_emit_nodes<<<blocks(I + S), T, 0, stream>>>(W.descs, S, I, W.inner_child, W.inner_range, W.inner_box,
+                                                  W.leaf_box, W.inner_height);
+    k_emit_atoms<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, W.vals_out);
+    return cuda_status(cudaGetLastError(), "LBVH build launch");
+}
+
+}  // namespace ehss

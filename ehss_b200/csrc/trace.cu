@@ -1,0 +1,578 @@
+// EHSS and PA kernels: nearest-entry query over the device LBVH, specular
+// bounce loop, any-hit PA, and the fused Sobol -> trace -> reduction blocks.
+//
+// Reference behaviour restated (paths relative to the reference project):
+//   nearest_scalar        src/support_exchange_transport/ehss_cpu.py:43-63
+//   _trace_loop           ehss_cpu.py:66-100, src/native/ehss_cpu.cpp:54-78
+//   entry_scalar/reflect  ehss_cpu.py:12-40 (see ehss_internal.cuh)
+//   tree_blocked / _one   pa_spatial.py:114-142 with sphere_hit inside_out_pa.py:93-101
+//   readout               ehss_state.py:84-103, ccs_cli.py:209-219
+//
+// Query design.  The reference walks a median-split tree in pre-order and
+// keeps the lexicographic (distance, atom id) minimum of the FP64 entry
+// distances.  Here a binary LBVH is walked near-child-first with a per-thread
+// stack; node boxes are FP32, rounded outward and expanded by eps_box, so a
+// box is culled only when it provably holds no entry at or before the
+// current bound U.  Two sphere-test precisions share the walk:
+//   EXACT (EHSS_PREC_FP64): every reached sphere is tested with the
+//     reference's FP64 formula; U is the running best distance rounded up.
+//   FILTER (EHSS_PREC_FP32): spheres are tested in FP32 with the
+//     cancellation-free perpendicular-distance discriminant
+//     disc = r^2 - |v - (v.d) d|^2 and a per-ray error bound (Ep on
+//     projections, Edisc on the discriminant).  Certain misses are dropped;
+//     certain hits give an interval [t - Et, t + Et] and lower U to t + Et;
+//     every sphere whose lower bound is <= U (certain or near-tangent) is
+//     kept in a 4-entry candidate list, re-tested in FP64 at the end with the
+//     reference formula and the (distance, id) rule.  The reached candidates
+//     always contain the FP64 winner, so outcomes equal EXACT's; a full list
+//     re-runs the query in EXACT mode.
+// Ray origins farther than 3 S from the structure centre (never produced by
+// the impact-disk source) use an FP64 all-atom search instead.
+#include <cstdio>
+#include "ehss_internal.cuh"
+
+namespace ehss {
+
+constexpr float kU32 = 5.9604645e-08f;   // 2^-24
+constexpr int kCand = 4;
+constexpr int kEmpty = INT32_MIN;
+constexpr int kSmemBins = 16;
+
+struct LocalStats {
+    uint32_t box, sphere, queries, grazing, fallback, fp64, errors;
+    __device__ LocalStats() : box(0), sphere(0), queries(0), grazing(0), fallback(0), fp64(0), errors(0) {}
+};
+
+struct RayF {
+    float ox, oy, oz, dx, dy, dz, ix, iy, iz, oix, oiy, oiz, Ep, Edisc;
+};
+
+__device__ __forceinline__ float safe_rcp(float x) {
+    float a = fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x;
+    return 1.0f / a;
+}
+
+// FP32 copy of an FP64 ray in the scene frame; false when the origin is too
+// far from the centre for the FP32 error bounds (or not finite).
+__device__ __forceinline__ bool setup_ray(const SceneHeader* H, const double* o, const double* d, RayF& r) {
+    r.ox = __double2float_rn(o[0] - H->center[0]);
+    r.oy = __double2float_rn(o[1] - H->center[1]);
+    r.oz = __double2float_rn(o[2] - H->center[2]);
+    r.dx = __double2float_rn(d[0]); r.dy = __double2float_rn(d[1]); r.dz = __double2float_rn(d[2]);
+    float S = H->scale_f;
+    float a = sqrtf(fmaf(r.ox, r.ox, fmaf(r.oy, r.oy, r.oz * r.oz)));
+    if (!(a <= 3.0f * S)) return false;
+    r.ix = safe_rcp(r.dx); r.iy = safe_rcp(r.dy); r.iz = safe_rcp(r.dz);
+    r.oix = r.ox * r.ix; r.oiy = r.oy * r.iy; r.oiz = r.oz * r.iz;
+    float A = a + S;
+    r.Ep = A * (32.0f * kU32);
+    float rm = H->rmax_f;
+    r.Edisc = (8.0f * kU32) * rm * rm + 2.5f * rm * r.Ep + 8.0f * r.Ep * r.Ep;
+    return true;
+}
+
+// Slab test of one child box against [0, U]; returns entry distance or +inf.
+__device__ __forceinline__ float box_enter(const RayF& r, float lx, float hx, float ly, float hy, float lz, float hz,
+                                           float U) {
+    float tlx = fmaf(lx, r.ix, -r.oix), thx = fmaf(hx, r.ix, -r.oix);
+    float tly = fmaf(ly, r.iy, -r.oiy), thy = fmaf(hy, r.iy, -r.oiy);
+    float tlz = fmaf(lz, r.iz, -r.oiz), thz = fmaf(hz, r.iz, -r.oiz);
+    float tmin = fmaxf(fmaxf(fminf(tlx, thx), fminf(tly, thy)), fmaxf(fminf(tlz, thz), 0.0f));
+    float tmax = fminf(fminf(fmaxf(tlx, thx), fmaxf(tly, thy)), fminf(fmaxf(tlz, thz), U));
+    return tmin <= tmax ? tmin : CUDART_INF_F;
+}
+
+// Reference rule of nearest_scalar (ehss_cpu.py:60): strictly nearer, or
+// equally near with a smaller input atom id.
+__device__ __forceinline__ bool better(double dist, int id, double best, int best_id) {
+    return dist < best || (dist == best && isfinite(dist) && (best_id < 0 || id < best_id));
+}
+
+// FP64 all-atom nearest search (origins far from the structure).
+__device__ int nearest_flat(const SceneView& S, const double* o, const double* d, int last_rank, double& best_out,
+                            LocalStats& st) {
+    int n = S.h->n_atoms;
+    double best = CUDART_INF;
+    int best_rank = -1, best_id = -1;
+    for (int k = 0; k < n; ++k) {
+        if (k == last_rank) continue;
+        double4 a = S.atoms64[k];
+        double t = entry64(o[0], o[1], o[2], d[0], d[1], d[2], a.x, a.y, a.z, a.w);
+        ++st.sphere; ++st.fp64;
+        int id = S.ids[k];
+        if (better(t, id, best, best_id)) { best = t; best_rank = k; best_id = id; }
+    }
+    best_out = best;
+    return best_rank;
+}
+
+// Nearest entry: returns the leaf-order rank of the collider (or -1) and its
+// FP64 entry distance, identical to the reference's choice.
+template <bool EXACT>
+__device__ int nearest(const SceneView& S, const double* o, const double* d, int last_rank, double& best_out,
+                       LocalStats& st) {
+    ++st.queries;
+    RayF r;
+    if (!setup_ray(S.h, o, d, r)) return nearest_flat(S, o, d, last_rank, best_out, st);
+    float U = CUDART_INF_F;
+    double best = CUDART_INF;
+    int best_rank = -1, best_id = -1;
+    int cand_rank[kCand];
+    float cand_lo[kCand];
+#pragma unroll
+    for (int e = 0; e < kCand; ++e) { cand_rank[e] = -1; cand_lo[e] = CUDART_INF_F; }
+    bool overflow = false, grazing = false;
+
+    int stack_ref[kStackDepth];
+    float stack_t[kStackDepth];
+    int sp = 0;
+    int cur = 0;
+    const int n_nodes = S.h->n_nodes, n_atoms = S.h->n_atoms;
+    // each node and leaf is entered at most once per query; more steps mean a malformed tree
+    for (int steps = 0;; ++steps) {
+        if (cur >= n_nodes || steps > 2 * n_nodes + 2) { ++st.errors; break; }
+        if (cur >= 0) {
+            const float4* nd = S.nodes + 4 * (int64_t)cur;
+            float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
+            st.box += 2;
+            float t0 = box_enter(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, U);
+            float t1 = box_enter(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, U);
+            int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+            bool h0 = t0 != CUDART_INF_F, h1 = t1 != CUDART_INF_F;
+            if (h0 && h1) {
+                bool swap = t1 < t0;
+                int nearc = swap ? c1 : c0, farc = swap ? c0 : c1;
+                float fart = swap ? t0 : t1;
+                if (sp < kStackDepth) { stack_ref[sp] = farc; stack_t[sp] = fart; ++sp; }
+                else { ++st.errors; }
+                cur = nearc;
+                continue;
+            }
+            if (h0) { cur = c0; continue; }
+            if (h1) { cur = c1; continue; }
+        } else if (cur != kEmpty) {
+            int code = ~cur;
+            int first = code >> 3, cnt = (code & 7) + 1;
+            if (first + cnt > n_atoms) { ++st.errors; cnt = 0; }
+            for (int k = first; k < first + cnt; ++k) {
+                if (k == last_rank) continue;
+                ++st.sphere;
+                if (EXACT) {
+                    double4 a = S.atoms64[k];
+                    double t = entry64(o[0], o[1], o[2], d[0], d[1], d[2], a.x, a.y, a.z, a.w);
+                    ++st.fp64;
+                    int id = __ldg(S.ids + k);
+                    if (better(t, id, best, best_id)) {
+                        best = t; best_rank = k; best_id = id;
+                        U = __double2float_ru(best);
+                    }
+                } else {
+                    float4 a = __ldg(S.atoms + k);
+                    float vx = a.x - r.ox, vy = a.y - r.oy, vz = a.z - r.oz;
+                    float b = fmaf(vx, r.dx, fmaf(vy, r.dy, vz * r.dz));
+                    float px = fmaf(-b, r.dx, vx), py = fmaf(-b, r.dy, vy), pz = fmaf(-b, r.dz, vz);
+                    float q = fmaf(px, px, fmaf(py, py, pz * pz));
+                    float disc = fmaf(a.w, a.w, -q);
+                    if (disc < -r.Edisc || b < -r.Ep) continue;          // certain miss
+                    float s = sqrtf(fmaxf(disc, 0.0f));
+                    float t = b - s;
+                    float lo;
+                    bool certain = false;
+                    if (disc >= 2.0f * r.Edisc) {
+                        float Et = 2.0f * (r.Ep + __fdividef(r.Edisc, s)) + 4.0f * kU32 * (fabsf(b) + s);
+                        if (t < -2.0f * Et) continue;                    // origin inside: no entry ahead
+                        if (t > Et) {
+                            certain = true;
+                            lo = t - Et;
+                            float up = t + Et;
+                            if (up < U) U = up;
+                        }
+                    }
+                    if (!certain) {
+                        lo = fmaxf(0.0f, (b - r.Ep - sqrtf(fmaxf(disc, 0.0f) + r.Edisc)) * (1.0f - 8.0f * kU32));
+                        grazing = true;
+                    }
+                    if (lo <= U) {
+                        bool placed = false;
+#pragma unroll
+                        for (int e = 0; e < kCand; ++e) {
+                            bool free_slot = cand_rank[e] < 0 || cand_lo[e] > U;
+                            if (!placed && free_slot) { cand_rank[e] = k; cand_lo[e] = lo; placed = true; }
+                        }
+                        if (!placed) overflow = true;
+                    }
+                }
+            }
+        }
+        // pop the nearest pending subtree that can still hold an entry <= U
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stack_t[sp] <= U) { cur = stack_ref[sp]; found = true; break; }
+        }
+        if (!found) break;
+    }
+    if (!EXACT) {
+        if (grazing) ++st.grazing;
+        if (overflow) {
+            ++st.fallback;
+            --st.queries;
+            return nearest<true>(S, o, d, last_rank, best_out, st);
+        }
+#pragma unroll
+        for (int e = 0; e < kCand; ++e) {
+            if (cand_rank[e] >= 0 && cand_lo[e] <= U) {
+                int k = cand_rank[e];
+                double4 a = S.atoms64[k];
+                double t = entry64(o[0], o[1], o[2], d[0], d[1], d[2], a.x, a.y, a.z, a.w);
+                ++st.fp64;
+                int id = __ldg(S.ids + k);
+                if (better(t, id, best, best_id)) { best = t; best_rank = k; best_id = id; }
+            }
+        }
+    }
+    best_out = best;
+    return best_rank;
+}
+
+// Any-hit PA query (pa_spatial._one with sphere_hit): true when the ray
+// meets any sphere other than owner_rank.
+__device__ bool anyhit(const SceneView& S, const double* o, const double* d, int owner_rank, LocalStats& st) {
+    ++st.queries;
+    RayF r;
+    if (!setup_ray(S.h, o, d, r)) {
+        int n = S.h->n_atoms;
+        for (int k = 0; k < n; ++k) {
+            if (k == owner_rank) continue;
+            double4 a = S.atoms64[k];
+            ++st.sphere; ++st.fp64;
+            if (sphere_hit64(o[0], o[1], o[2], d[0], d[1], d[2], a.x, a.y, a.z, a.w)) return true;
+        }
+        return false;
+    }
+    int stack_ref[kStackDepth];
+    int sp = 0;
+    int cur = 0;
+    const float U = CUDART_INF_F;
+    const int n_nodes = S.h->n_nodes, n_atoms = S.h->n_atoms;
+    for (int steps = 0;; ++steps) {
+        if (cur >= n_nodes || steps > 2 * n_nodes + 2) { ++st.errors; break; }
+        if (cur >= 0) {
+            const float4* nd = S.nodes + 4 * (int64_t)cur;
+            float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
+            st.box += 2;
+            bool h0 = box_enter(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, U) != CUDART_INF_F;
+            bool h1 = box_enter(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, U) != CUDART_INF_F;
+            int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+            if (h0 && h1) {
+                if (sp < kStackDepth) stack_ref[sp++] = c1; else ++st.errors;
+                cur = c0;
+                continue;
+            }
+            if (h0) { cur = c0; continue; }
+            if (h1) { cur = c1; continue; }
+        } else if (cur != kEmpty) {
+            int code = ~cur;
+            int first = code >> 3, cnt = (code & 7) + 1;
+            if (first + cnt > n_atoms) { ++st.errors; cnt = 0; }
+            for (int k = first; k < first + cnt; ++k) {
+                if (k == owner_rank) continue;
+                ++st.sphere;
+                float4 a = __ldg(S.atoms + k);
+                float vx = a.x - r.ox, vy = a.y - r.oy, vz = a.z - r.oz;
+                float b = fmaf(vx, r.dx, fmaf(vy, r.dy, vz * r.dz));
+                float px = fmaf(-b, r.dx, vx), py = fmaf(-b, r.dy, vy), pz = fmaf(-b, r.dz, vz);
+                float q = fmaf(px, px, fmaf(py, py, pz * pz));
+                float disc = fmaf(a.w, a.w, -q);
+                if (disc < -r.Edisc) continue;
+                float s = sqrtf(fmaxf(disc, 0.0f));
+                float exitp = b + s;     // far root: the reference's -b + sqrt(disc) with b = x.d = -(v.d)
+                if (disc >= 2.0f * r.Edisc) {
+                    float Et = 2.0f * (r.Ep + __fdividef(r.Edisc, s)) + 4.0f * kU32 * (fabsf(b) + s);
+                    if (exitp > Et) return true;
+                    if (exitp < -2.0f * Et) continue;
+                } else if (b + sqrtf(fmaxf(disc, 0.0f) + r.Edisc) < -2.0f * r.Ep) {
+                    continue;
+                }
+                double4 a64 = S.atoms64[k];
+                ++st.fp64;
+                if (sphere_hit64(o[0], o[1], o[2], d[0], d[1], d[2], a64.x, a64.y, a64.z, a64.w)) return true;
+            }
+        }
+        if (sp == 0) break;
+        cur = stack_ref[--sp];
+    }
+    return false;
+}
+
+struct TraceOut {
+    int64_t bounces;
+    bool escaped, unresolved;
+};
+
+// _trace_loop body for one ray (ehss_cpu.py:72-98).  o/d are updated in
+// place; history (may be null) receives input atom ids.
+__device__ __forceinline__ TraceOut trace_ray(const SceneView& S, double* o, double* d, int last_rank,
+                                              int64_t count, int cap, bool exact, int32_t* history,
+                                              LocalStats& st) {
+    TraceOut out;
+    out.escaped = out.unresolved = false;
+    while (true) {
+        double best;
+        int k = exact ? nearest<true>(S, o, d, last_rank, best, st) : nearest<false>(S, o, d, last_rank, best, st);
+        if (k < 0) { out.escaped = true; break; }
+        if (count >= cap) { out.unresolved = true; break; }
+        double4 a = S.atoms64[k];
+        reflect64(o[0], o[1], o[2], d[0], d[1], d[2], a.x, a.y, a.z, a.w, best);
+        if (history) history[count] = S.ids[k];
+        ++count;
+        last_rank = k;
+    }
+    out.bounces = count;
+    return out;
+}
+
+__device__ __forceinline__ void flush_stats(const LocalStats& st, uint64_t* stats) {
+    if (!stats) return;
+    unsigned v[7] = {st.box, st.sphere, st.queries, st.grazing, st.fallback, st.fp64, st.errors};
+    const int slot[7] = {EHSS_STAT_BOX_TESTS, EHSS_STAT_SPHERE_TESTS, EHSS_STAT_QUERIES, EHSS_STAT_GRAZING,
+                         EHSS_STAT_FALLBACK, EHSS_STAT_FP64_TESTS, EHSS_STAT_ERRORS};
+    unsigned lane = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        // 64-bit warp sum (per-thread counts can exceed 2^32 / 32 on long runs)
+        unsigned long long x = v[i];
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+        if (lane == 0 && x) atomicAdd((unsigned long long*)&stats[slot[i]], x);
+    }
+}
+
+// --------------------------------------------------------------------------
+// Explicit-ray kernels
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_trace_rays(const void* scene, int64_t n, int cap, int exact, double* P,
+                                                    double* D, const int64_t* last_atom, int64_t* bounces,
+                                                    uint8_t* escaped, uint8_t* unresolved, int32_t* history,
+                                                    uint64_t* stats) {
+    SceneView S = scene_view(scene);
+    LocalStats st;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t first = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool ok = S.h->magic == kSceneMagic && S.h->status == 0;
+    for (int64_t i = first; i < n; i += stride) {
+        double o[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
+        double d[3] = {D[3 * i], D[3 * i + 1], D[3 * i + 2]};
+        int64_t count = bounces[i];
+        int64_t last_id = last_atom[i];
+        int32_t* h = history ? history + i * (int64_t)cap : nullptr;
+        if (!ok || last_id < -1 || last_id >= S.h->n_atoms || count < 0 || count > 1 ||
+            (count == 1 && last_id < 0)) {
+            ++st.errors;
+            escaped[i] = 0; unresolved[i] = 0;
+            continue;
+        }
+        int last_rank = last_id >= 0 ? S.rank[last_id] : -1;
+        if (h && count == 1) h[0] = (int32_t)last_id;
+        TraceOut t = trace_ray(S, o, d, last_rank, count, cap, exact != 0, h, st);
+        P[3 * i] = o[0]; P[3 * i + 1] = o[1]; P[3 * i + 2] = o[2];
+        D[3 * i] = d[0]; D[3 * i + 1] = d[1]; D[3 * i + 2] = d[2];
+        bounces[i] = t.bounces;
+        escaped[i] = t.escaped;
+        unresolved[i] = t.unresolved;
+    }
+    flush_stats(st, stats);
+}
+
+__global__ void __launch_bounds__(128) k_pa_rays(const void* scene, int64_t n, const double* P, const double* D,
+                                                 const int64_t* owners, uint8_t* blocked, uint64_t* stats) {
+    SceneView S = scene_view(scene);
+    LocalStats st;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool ok = S.h->magic == kSceneMagic && S.h->status == 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+        double o[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
+        double d[3] = {D[3 * i], D[3 * i + 1], D[3 * i + 2]};
+        int64_t owner = owners ? owners[i] : -1;
+        if (!ok || owner < -1 || owner >= S.h->n_atoms) { ++st.errors; blocked[i] = 0; continue; }
+        blocked[i] = anyhit(S, o, d, owner >= 0 ? S.rank[owner] : -1, st);
+    }
+    flush_stats(st, stats);
+}
+
+__global__ void k_sobol_points(int dim, SobolParams p, int64_t first, int64_t n, uint32_t* q) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t idx = (uint32_t)(first + i);
+    uint32_t g = idx ^ (idx >> 1);
+    for (int j = 0; j < dim; ++j) {
+        uint32_t v = p.shift[j];
+        uint32_t gg = g;
+        while (gg) {
+            int k = __ffs(gg) - 1;
+            gg &= gg - 1;
+            v ^= p.sv[j * 30 + k];
+        }
+        q[i * dim + j] = v;
+    }
+}
+
+__global__ void k_source_rays(const void* scene, Sobol4Params p, int64_t first, int64_t n, double* O, double* Dd) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    SceneView S = scene_view(scene);
+    uint4 q = sobol4(p.sv, p.shift, (uint32_t)(first + i));
+    Ray64 ray = impact_ray(q, S.h->center, S.h->radius);
+    for (int c = 0; c < 3; ++c) { O[3 * i + c] = ray.o[c]; Dd[3 * i + c] = ray.d[c]; }
+}
+
+// --------------------------------------------------------------------------
+// Fused blocks (persistent): Sobol -> impact disk -> EHSS / PA -> reduction
+// --------------------------------------------------------------------------
+struct WarpBins {
+    unsigned count[kSmemBins];
+    unsigned long long ledger[kSmemBins];
+};
+
+__device__ __forceinline__ unsigned long long warp_sum64(unsigned long long x) {
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+    return x;
+}
+
+__global__ void __launch_bounds__(256) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
+                                                int chunk_rays, ehss_block_result* results, uint64_t* hist,
+                                                uint64_t* ledger, unsigned long long* work) {
+    extern __shared__ WarpBins bins_all[];
+    const unsigned lane = threadIdx.x & 31;
+    WarpBins& bins = bins_all[threadIdx.x >> 5];
+    while (true) {
+        long long c = 0;
+        if (lane == 0) c = (long long)atomicAdd(work, 1ull);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= total_chunks) break;
+        // block owning chunk c: last b with chunk_begin <= c
+        int lo = 0, hi = nb - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (blocks[mid].chunk_begin <= c) lo = mid; else hi = mid - 1;
+        }
+        const ehss_block* B = blocks + lo;
+        const int log2n = B->log2_rays, cap = B->cap;
+        const uint32_t flags = B->flags;
+        const bool exact = B->precision == EHSS_PREC_FP64;
+        const int64_t n_rays = 1ll << log2n;
+        const int64_t ray0 = (c - B->chunk_begin) * (int64_t)chunk_rays;
+        const int64_t cnt = min((int64_t)chunk_rays, n_rays - ray0);
+        const uint4* sv = reinterpret_cast<const uint4*>(B->sv);
+        const uint4 shift = make_uint4(B->shift[0], B->shift[1], B->shift[2], B->shift[3]);
+        SceneView S = scene_view(B->scene);
+        const bool ok = S.h->magic == kSceneMagic && S.h->status == 0;
+        const double center[3] = {S.h->center[0], S.h->center[1], S.h->center[2]};
+        const double radius = S.h->radius;
+        if (lane < kSmemBins) { bins.count[lane] = 0; bins.ledger[lane] = 0; }
+        __syncwarp();
+        LocalStats st;
+        unsigned long long acc_fx = 0;
+        unsigned n_hits = 0, n_unres = 0, n_esc = 0, n_pa = 0;
+        for (int64_t j = lane; j < cnt && ok; j += 32) {
+            uint32_t idx = (uint32_t)(ray0 + j);
+            Ray64 ray = impact_ray(sobol4(sv, shift, idx), center, radius);
+            if (flags & EHSS_BLOCK_PA) n_pa += anyhit(S, ray.o, ray.d, -1, st);
+            if (flags & EHSS_BLOCK_EHSS) {
+                double din[3] = {ray.d[0], ray.d[1], ray.d[2]};
+                TraceOut t = trace_ray(S, ray.o, ray.d, -1, 0, cap, exact, nullptr, st);
+                unsigned long long fx = 0;
+                if (t.escaped) {
+                    double a = scatter_angle(din[0], din[1], din[2], ray.d[0], ray.d[1], ray.d[2]);
+                    fx = __double2ull_rn(a * 0x1p40);
+                    ++n_esc;
+                }
+                acc_fx += fx;
+                n_hits += (t.bounces > 0) || t.unresolved;
+                n_unres += t.unresolved;
+                int64_t k = t.bounces;
+                if (k < kSmemBins) {
+                    atomicAdd(&bins.count[k], 1u);
+                    if (fx) atomicAdd(&bins.ledger[k], fx);
+                } else {
+                    atomicAdd((unsigned long long*)&hist[B->hist_offset + k], 1ull);
+                    if (fx) atomicAdd((unsigned long long*)&ledger[B->hist_offset + k], fx);
+                }
+            }
+        }
+        if (!ok && lane == 0) ++st.errors;
+        // warp reduction of the chunk, then one atomic per field into the block result
+        unsigned long long s_fx = warp_sum64(acc_fx);
+        unsigned s_hits = __reduce_add_sync(0xffffffffu, n_hits);
+        unsigned s_unres = __reduce_add_sync(0xffffffffu, n_unres);
+        unsigned s_esc = __reduce_add_sync(0xffffffffu, n_esc);
+        unsigned s_pa = __reduce_add_sync(0xffffffffu, n_pa);
+        ehss_block_result* R = results + lo;
+        if (lane == 0) {
+            if (s_fx) atomicAdd((unsigned long long*)&R->angle_fx, s_fx);
+            if (s_hits) atomicAdd((unsigned long long*)&R->hits, (unsigned long long)s_hits);
+            if (s_unres) atomicAdd((unsigned long long*)&R->unresolved, (unsigned long long)s_unres);
+            if (s_esc) atomicAdd((unsigned long long*)&R->escaped, (unsigned long long)s_esc);
+            if (s_pa) atomicAdd((unsigned long long*)&R->pa_blocked, (unsigned long long)s_pa);
+        }
+        flush_stats(st, R->stats);
+        __syncwarp();
+        if (lane < kSmemBins && lane <= cap) {
+            if (bins.count[lane])
+                atomicAdd((unsigned long long*)&hist[B->hist_offset + lane], (unsigned long long)bins.count[lane]);
+            if (bins.ledger[lane]) atomicAdd((unsigned long long*)&ledger[B->hist_offset + lane], bins.ledger[lane]);
+        }
+        __syncwarp();
+    }
+}
+
+// --------------------------------------------------------------------------
+// Host launchers
+// --------------------------------------------------------------------------
+static unsigned grid_for(int64_t n, int threads) {
+    int64_t want = (n + threads - 1) / threads;
+    int64_t cap = (int64_t)sm_count() * 16;
+    if (want > cap) want = cap;
+    return (unsigned)(want > 0 ? want : 1);
+}
+
+int launch_trace_rays(const void* scene, int64_t n, int cap, int precision, double* P, double* D,
+                      const int64_t* last, int64_t* bounces, uint8_t* esc, uint8_t* unres, int32_t* hist,
+                      uint64_t* stats, cudaStream_t stream) {
+    if (n == 0) return EHSS_OK;
+    k_trace_rays<<<grid_for(n, 128), 128, 0, stream>>>(scene, n, cap, precision == EHSS_PREC_FP64, P, D, last,
+                                                       bounces, esc, unres, hist, stats);
+    return cuda_status(cudaGetLastError(), "trace launch");
+}
+
+int launch_pa_rays(const void* scene, int64_t n, const double* P, const double* D, const int64_t* owners,
+                   uint8_t* blocked, uint64_t* stats, cudaStream_t stream) {
+    if (n == 0) return EHSS_OK;
+    k_pa_rays<<<grid_for(n, 128), 128, 0, stream>>>(scene, n, P, D, owners, blocked, stats);
+    return cuda_status(cudaGetLastError(), "PA launch");
+}
+
+int launch_sobol_points(int dim, const SobolParams& p, int64_t first, int64_t n, uint32_t* q, cudaStream_t stream) {
+    if (n == 0) return EHSS_OK;
+    k_sobol_points<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(dim, p, first, n, q);
+    return cuda_status(cudaGetLastError(), "Sobol launch");
+}
+
+int launch_source_rays(const void* scene, const Sobol4Params& p, int64_t first, int64_t n, double* O, double* D,
+                       cudaStream_t stream) {
+    if (n == 0) return EHSS_OK;
+    k_source_rays<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(scene, p, first, n, O, D);
+    return cuda_status(cudaGetLastError(), "source launch");
+}
+
+int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const ehss_launch& L,
+                  ehss_block_result* results, uint64_t* hist, uint64_t* ledger, unsigned long long* work,
+                  cudaStream_t stream) {
+    int warps = L.block_threads / 32;
+    size_t smem = sizeof(WarpBins) * (size_t)warps;
+    unsigned grid = (unsigned)(sm_count() * L.ctas_per_sm);
+    k_blocks<<<grid, L.block_threads, smem, stream>>>(blocks, nb, total_chunks, L.chunk_rays, results, hist, ledger,
+                                                      work);
+    return cuda_status(cudaGetLastError(), "blocks launch");
+}
+
+}  // namespace ehss

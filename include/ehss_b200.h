@@ -1,0 +1,209 @@
+/*
+ * ehss_b200 — C ABI of the B200 (sm_100a) PA + EHSS cross-section library.
+ *
+ * Every entry point returns an int status (EHSS_OK = 0) and never aborts;
+ * ehss_last_error() gives the message of the calling thread's last failure.
+ * Array arguments named *_dev are device pointers (any allocator: PyTorch,
+ * cudaMalloc, a pool); *_host are host pointers.  `stream` is a cudaStream_t
+ * passed as void* (NULL = legacy default stream).  Work is enqueued on that
+ * stream; nothing synchronises unless the comment says so.
+ *
+ * The reference (SCIMMS/EHSS, package support_exchange_transport) exposes
+ * this path as Python objects plus one native C entry point; each function
+ * below names the reference interface it replaces (paths relative to the
+ * reference project root).
+ */
+#ifndef EHSS_B200_H
+#define EHSS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EHSS_ABI_VERSION 1
+
+/* Status codes.  EHSS_ERR_VALUE corresponds to the reference's ValueError. */
+#define EHSS_OK 0
+#define EHSS_ERR_VALUE 1    /* invalid argument (size, cap, identity, layout) */
+#define EHSS_ERR_CUDA 2     /* a CUDA runtime call failed */
+#define EHSS_ERR_CAPACITY 3 /* a buffer or workspace is too small */
+#define EHSS_ERR_DEVICE 4   /* a kernel reported a bounded failure (stack/loop limit) */
+
+/* Precision of the nearest-entry search. */
+#define EHSS_PREC_FP64 0    /* every sphere test in FP64, bit-identical to the reference */
+#define EHSS_PREC_FP32 1    /* FP32 traversal + tests, FP64 re-test of every candidate that
+                               can be nearest (same outcomes as FP64 by construction) */
+
+/* Per-call statistics slots (uint64 array of EHSS_NSTATS, accumulated). */
+#define EHSS_STAT_BOX_TESTS 0
+#define EHSS_STAT_SPHERE_TESTS 1
+#define EHSS_STAT_QUERIES 2
+#define EHSS_STAT_GRAZING 3      /* queries whose FP32 tangency/order margin was below the
+                                    error bound, resolved by the FP64 re-test */
+#define EHSS_STAT_FALLBACK 4     /* queries re-run entirely in FP64 (candidate list full) */
+#define EHSS_STAT_FP64_TESTS 5   /* FP64 sphere evaluations */
+#define EHSS_STAT_ERRORS 6       /* bounded device failures (must stay 0) */
+#define EHSS_NSTATS 8
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* ehss_last_error(void);
+int ehss_abi_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Scrambled Sobol (host).  Replaces scipy qmc.Sobol(dim, scramble=True,
+ * seed=seed) as called by ehss_state.external_source
+ * (src/support_exchange_transport/ehss_state.py:44) and ccs_cli.adaptive_pa
+ * (ccs_cli.py:148): sv[dim*30] receives the LMS-scrambled direction numbers
+ * (row j = dimension j), shift[dim] the random digital shift; point n is
+ * (shift ^ XOR_{bit k of gray(n)} sv[k]) * 2^-30.  1 <= dim <= 8,
+ * seed < 2^64. */
+int ehss_sobol_scramble(int dim, uint64_t seed, uint32_t* sv_host, uint32_t* shift_host);
+
+/* The same points generated on the device: q_dev[n*dim] (uint32, row-major)
+ * for point indices [first, first+n).  Bit-exact to scipy's sequence. */
+int ehss_sobol_points(int dim, uint64_t seed, int64_t first, int64_t n, uint32_t* q_dev, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Scene: one structure's atoms plus a device LBVH, resident in a caller-
+ * owned device buffer.  Replaces PreparedStaticCPUEHSS.__init__
+ * (ehss_static.py:62-101) and SphereIndex.__init__ (pa_spatial.py:157-160):
+ * the scene owns a copy of the coordinates (as the reference scene does,
+ * ehss_static.py:68-69).  Results never depend on the tree.  leaf_size 1..8
+ * is the LBVH leaf bound (the reference's --leaf-size only shapes its own
+ * tree and has no effect on results). */
+typedef struct ehss_scene_info {
+    int64_t n_atoms;
+    int64_t n_nodes;
+    int32_t leaf_size;
+    int32_t depth;            /* LBVH depth (root = 1) */
+    double center[3];         /* sequential mean of the centres (ehss_state.py:46) */
+    double radius;            /* impact-disk radius R (ehss_state.py:47) */
+    double scale;             /* max |c_j - center| + r_j */
+    double rmax;              /* largest radius */
+    uint64_t bytes;           /* bytes used in the scene buffer */
+} ehss_scene_info;
+
+/* Bytes of the scene buffer and of the build workspace for n_atoms. */
+int ehss_scene_bytes(int64_t n_atoms, int leaf_size, uint64_t* scene_bytes, uint64_t* workspace_bytes);
+
+/* Build a scene from device arrays xyz_dev[n*3] and radii_dev[n] (float64,
+ * Angstrom).  scene_dev and workspace_dev must be 256-byte aligned.  Radii
+ * must be positive and finite (checked on the device; failures are reported
+ * by ehss_scene_info). */
+int ehss_scene_build(int64_t n_atoms, const double* xyz_dev, const double* radii_dev, int leaf_size,
+                     void* scene_dev, uint64_t scene_bytes, void* workspace_dev, uint64_t workspace_bytes,
+                     void* stream);
+
+/* Batched build: n_scenes structures in one pass of the builder kernels
+ * (the batched/served forms build every admitted structure at once).
+ * Arrays of device pointers and sizes are host arrays of length n_scenes. */
+int ehss_scenes_workspace_bytes(int n_scenes, const int64_t* n_atoms_host, uint64_t* workspace_bytes);
+int ehss_scenes_build(int n_scenes, const double* const* xyz_dev, const double* const* radii_dev,
+                      const int64_t* n_atoms_host, int leaf_size, void* const* scenes_dev,
+                      const uint64_t* scene_bytes_host, void* workspace_dev, uint64_t workspace_bytes,
+                      void* stream);
+
+/* Copy the scene header to the host (synchronises `stream`).  Fails with
+ * EHSS_ERR_VALUE when the build found a non-positive or non-finite radius or
+ * a non-finite coordinate. */
+int ehss_scene_info_get(const void* scene_dev, ehss_scene_info* info_host, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Impact-disk source on the device.  Replaces ehss_state.external_source
+ * (ehss_state.py:42-53): 2^log2n rays from Sobol(4, seed); writes origins and
+ * directions (float64 [n*3]) for ray indices [first, first+n).  Each ray's
+ * weight is pi*R*R/2^log2n with R from ehss_scene_info. */
+int ehss_source_rays(const void* scene_dev, int log2n, uint64_t seed, int64_t first, int64_t n,
+                     double* origins_dev, double* directions_dev, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* EHSS trace of explicit rays.  Replaces the reference's native entry point
+ * ehss_trace (src/native/ehss_cpu.cpp:42-82) and CPUEHSSTransport.trace
+ * (ehss_cpu.py:118-142): positions_dev/directions_dev [n*3] hold the source
+ * origins/directions on entry and the final positions/outgoing directions on
+ * return; bounces_dev holds the initial bounce count (0 or 1) on entry and the
+ * collision count on return; last_atom_dev is the initial collider (-1 for
+ * none).  escaped/unresolved are 0/1 bytes.  history_dev is NULL or an
+ * int32 [n*cap] array that receives collider ids (-1 filled), as
+ * record_history does.  stats_dev (NULL or uint64[EHSS_NSTATS]) is
+ * accumulated.  cap >= 1. */
+int ehss_trace(const void* scene_dev, int64_t n_rays, int cap, int precision,
+               double* positions_dev, double* directions_dev, const int64_t* last_atom_dev,
+               int64_t* bounces_dev, uint8_t* escaped_dev, uint8_t* unresolved_dev, int32_t* history_dev,
+               uint64_t* stats_dev, void* stream);
+
+/* BVH any-hit PA of explicit rays.  Replaces SphereIndex.query / tree_blocked
+ * (pa_spatial.py:133-142, 162-164) with sphere_hit semantics
+ * (inside_out_pa.py:93-101): blocked_dev[i] = 1 when ray i meets a sphere
+ * other than owners_dev[i] (NULL = no owner). */
+int ehss_pa_anyhit(const void* scene_dev, int64_t n_rays, const double* origins_dev, const double* directions_dev,
+                   const int64_t* owners_dev, uint8_t* blocked_dev, uint64_t* stats_dev, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Fused blocks: Sobol -> impact disk -> trace -> (1 - cos chi) reduction,
+ * with no per-ray HBM traffic.  One block = one replicate of one structure
+ * (the body of ccs_cli.solve_frame's repeat loop, ccs_cli.py:189-219).  The
+ * same entry point serves one structure (plain path) and many structures of
+ * uneven size in one persistent launch (batched path).
+ *
+ * Sums are kept in integer fixed point so that every block's result is
+ * independent of scheduling and of what else runs in the launch:
+ *   omega     = w * angle_fx * 2^-40        (w = pi R^2 / 2^log2_rays)
+ *   pa (same rays) = w * hits ;  tail bound = 2 * w * unresolved
+ * hist/ledger rows have cap+1 entries (bincount of bounces, unweighted and
+ * weighted by the contribution in 2^-40 units). */
+#define EHSS_BLOCK_EHSS 1u      /* trace EHSS */
+#define EHSS_BLOCK_PA 2u        /* any-hit PA on the same rays */
+
+typedef struct ehss_block {
+    const void* scene;        /* device scene buffer */
+    uint32_t sv[30][4];       /* Sobol(4) direction numbers, [bit][dim] */
+    uint32_t shift[4];
+    int32_t log2_rays;        /* 3..24 */
+    int32_t cap;              /* collision cap >= 1 */
+    int32_t precision;        /* EHSS_PREC_* */
+    uint32_t flags;           /* EHSS_BLOCK_* */
+    int64_t hist_offset;      /* first hist/ledger entry of this block */
+    int64_t chunk_begin;      /* filled by ehss_blocks_prepare */
+} ehss_block;
+
+typedef struct ehss_block_result {
+    uint64_t angle_fx;        /* sum of clip(1 - d_in.d_out, 0, 2) over escaped rays, 2^-40 units */
+    uint64_t hits;            /* rays with bounces > 0 or unresolved */
+    uint64_t unresolved;
+    uint64_t escaped;
+    uint64_t pa_blocked;      /* any-hit PA count (EHSS_BLOCK_PA) */
+    uint64_t stats[EHSS_NSTATS];
+} ehss_block_result;
+
+/* Fill seeds' scrambles and chunk offsets of host block descriptors; returns
+ * the total chunk count.  chunk_rays is a power of two (32..4096). */
+int ehss_blocks_prepare(ehss_block* blocks_host, int n_blocks, const uint64_t* seeds_host, int chunk_rays,
+                        int64_t* total_chunks);
+
+/* Workspace bytes for ehss_trace_blocks. */
+int ehss_blocks_workspace_bytes(int n_blocks, uint64_t* bytes);
+
+/* Launch configuration chosen by the caller or the autotuner. */
+typedef struct ehss_launch {
+    int32_t block_threads;    /* 64..256, multiple of 32 */
+    int32_t ctas_per_sm;      /* persistent CTAs per SM (grid = SMs * ctas_per_sm) */
+    int32_t chunk_rays;       /* rays per work item (as passed to ehss_blocks_prepare); each
+                                 lane of the warp that takes the item traces chunk_rays/32 rays */
+    int32_t reserved;         /* 0 */
+} ehss_launch;
+
+/* Run all blocks in one persistent launch.  blocks_dev: device copy of the
+ * prepared descriptors; results_dev[n_blocks], hist_dev/ledger_dev
+ * [sum of (cap+1)] are zeroed by this call before accumulation. */
+int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks,
+                      ehss_block_result* results_dev, uint64_t* hist_dev, uint64_t* ledger_dev,
+                      int64_t hist_entries, void* workspace_dev, uint64_t workspace_bytes,
+                      const ehss_launch* launch, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EHSS_B200_H */

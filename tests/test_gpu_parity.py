@@ -1,0 +1,303 @@
+"""CUDA path against the CPU oracle and the reference's golden fixtures.
+
+All tests call libehss_b200.so through its C ABI (via the ehss_b200 Python
+objects) on a B200.  Integer, index and per-ray FP64 outcomes must be
+bit-identical; CCS sums (integer fixed point on the device) must agree with the
+oracle's FP64 sums to 1e-12 relative, far inside the 1e-5 CCS bound.
+"""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TRACE_CASES = ['cloud37', 'cloud37_rev', 'trap', 'single', 'impact', 'pub4', 'cap1', 'triatomic', 'cloud300',
+               'cloud300_leaf1', 'translated']
+CCS_RTOL = 1e-12
+
+
+@pytest.fixture(scope='module')
+def eb():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    import ehss_b200
+    from ehss_b200 import _lib
+    _lib.load()
+    return ehss_b200
+
+
+def _source(g, name):
+    from ehss_b200 import EHSSSource
+    return EHSSSource(g[name + '_origins'], g[name + '_directions'], g[name + '_incoming'], g[name + '_weights'],
+                      g[name + '_last_atom'], g[name + '_initial'], 'fixture')
+
+
+def _assert_same_paths(r, g, name, cap):
+    for field in ('positions', 'outgoing'):
+        np.testing.assert_array_equal(getattr(r, field), g[f'{name}_{field}'], err_msg=f'{name} {field}')
+    for field in ('escaped', 'unresolved', 'bounces'):
+        np.testing.assert_array_equal(getattr(r, field), g[f'{name}_{field}'], err_msg=f'{name} {field}')
+    width = g[name + '_collider_ids'].shape[1]
+    np.testing.assert_array_equal(r.collider_ids[:, :width], g[name + '_collider_ids'], err_msg=name)
+    assert (r.collider_ids[:, width:] == -1).all()
+
+
+def test_device_sobol_bit_exact(eb, golden):
+    import torch
+    from ehss_b200 import _lib
+    from ehss_b200.device import stream_handle
+    lib = _lib.load()
+    g = golden('sobol.npz')
+    for key in sorted({k.rsplit('_', 1)[0] for k in g if k.startswith('d')}):
+        d, m, s = (int(part[1:]) for part in key.split('_'))
+        n = 1 << m
+        q = torch.empty(n * d, dtype=torch.int32, device='cuda')
+        _lib.check(lib.ehss_sobol_points(d, s, 0, n, q.data_ptr(), stream_handle()))
+        got = q.cpu().numpy().view(np.uint32).reshape(n, d)
+        np.testing.assert_array_equal(got, g[key + '_q'], err_msg=key)
+    # an offset window of the sequence
+    q = torch.empty(100 * 4, dtype=torch.int32, device='cuda')
+    _lib.check(lib.ehss_sobol_points(4, 7, 1000, 100, q.data_ptr(), stream_handle()))
+    np.testing.assert_array_equal(q.cpu().numpy().view(np.uint32).reshape(100, 4),
+                                  O.sobol_integers(4, 11, 7)[1000:1100])
+
+
+def test_scene_center_and_radius_bit_exact(eb, golden):
+    g = golden('trace.npz')
+    for name in ('cloud37', 'cloud300', 'translated', 'single', 'triatomic'):
+        c, r = g[name + '_centers'], g[name + '_radii']
+        scene = eb.Scene(c, r)
+        center, radius = O.enclosing(c, r)
+        np.testing.assert_array_equal(scene.center, center)
+        assert scene.radius == radius
+
+
+def test_device_source_matches_numpy_mapping(eb, golden):
+    g = golden('source.npz')
+    for name in ('pub4', 'single', 'tri'):
+        c, r = g[name + '_centers'], g[name + '_radii']
+        m, s = int(g[name + '_m']), int(g[name + '_seed'])
+        src = eb.external_source(eb.Spheres(c, r, deduplicate=False), m, s)
+        np.testing.assert_array_equal(src.weights, g[name + '_weights'])
+        # cos/sin differ from numpy by ulps only
+        np.testing.assert_allclose(src.directions, g[name + '_directions'], rtol=0, atol=4e-16)
+        np.testing.assert_allclose(src.origins, g[name + '_origins'], rtol=0, atol=1e-13 * (1 + np.abs(c).max()))
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+@pytest.mark.parametrize('name', TRACE_CASES)
+def test_trace_bit_exact_on_reference_rays(eb, golden, name, precision):
+    g = golden('trace.npz')
+    s = eb.Spheres(g[name + '_centers'], g[name + '_radii'], deduplicate=False)
+    cap = int(g[name + '_cap'])
+    eng = eb.PreparedStaticGPUEHSS(s, leaf_size=int(g[name + '_leaf']), precision=precision).engine
+    r = eng.trace(_source(g, name), cap, record_history=True)
+    _assert_same_paths(r, g, name, cap)
+    assert r.omega == pytest.approx(float(g[name + '_omega']), rel=1e-15, abs=1e-300)
+    assert r.tail_bound == float(g[name + '_tail'])
+    assert r.pa == float(g[name + '_pa'])
+    assert r.metrics['fp64_fallback_queries'] >= 0
+
+
+@pytest.mark.parametrize('leaf', [1, 2, 4, 8])
+def test_trace_matches_oracle_on_globule_device_rays(eb, leaf):
+    from ehss_b200 import workloads as W
+    c, r, _ = W.globule(650, 11)
+    s = eb.Spheres(c, r, deduplicate=False)
+    prep = eb.PreparedStaticGPUEHSS(s, leaf_size=leaf, precision='fp32')
+    src = eb.external_source(s, 12, 5, scene=prep.scene)
+    got = prep.engine.trace(src, 64, record_history=True)
+    tree = O.StaticTree(c, r, 4)
+    ref = tree.trace(src.origins, src.directions, cap=64, record=True, threads=4)
+    for field in ('positions', 'outgoing', 'escaped', 'unresolved', 'bounces', 'collider_ids'):
+        np.testing.assert_array_equal(getattr(got, field), ref[field], err_msg=field)
+    exact = eb.PreparedStaticGPUEHSS(s, leaf_size=leaf, precision='fp64').engine.trace(src, 64, record_history=True)
+    np.testing.assert_array_equal(exact.outgoing, got.outgoing)
+
+
+def test_fp32_and_fp64_agree_on_dense_globule_with_grazing_stats(eb):
+    from ehss_b200 import workloads as W
+    c, r, _ = W.globule(2000, 3)
+    s = eb.Spheres(c, r, deduplicate=False)
+    prep = eb.PreparedStaticGPUEHSS(s, precision='fp32')
+    src = eb.external_source(s, 14, 9, scene=prep.scene)
+    a = prep.engine.trace(src, 64)
+    b = eb.GPUEHSSTransport(prep.scene, precision='fp64').trace(src, 64)
+    disagree = np.count_nonzero((a.bounces != b.bounces) | (a.escaped != b.escaped)
+                                | np.any(a.outgoing != b.outgoing, axis=1))
+    assert disagree == 0
+    assert a.metrics['queries'] > 0
+    assert abs(a.omega - b.omega) <= 1e-14 * b.omega
+
+
+def test_fused_blocks_match_oracle_readout(eb):
+    from ehss_b200 import workloads as W
+    from ehss_b200.blocks import BlockJob, BlockPlan
+    c, r, _ = W.globule(650, 21)
+    scene = eb.Scene(c, r)
+    tree = O.StaticTree(c, r, 4)
+    jobs = [BlockJob(scene, 12, seed, cap=cap, precision=p, pa=True, tag=(seed, cap, p))
+            for seed in (0, 1) for cap in (1, 64) for p in (0, 1)]
+    plan = BlockPlan(jobs)
+    plan.run()
+    res = plan.collect()
+    pat = O.PATree(c, r, 4)
+    for job, got in zip(jobs, res):
+        o, d = scene.source_rays(job.log2_rays, job.seed)
+        src = dict(origins=o.cpu().numpy(), directions=d.cpu().numpy())
+        src['incoming'] = src['directions'].copy()
+        n = len(src['origins'])
+        src['weights'] = np.full(n, np.pi * scene.radius ** 2 / n)
+        ref = tree.trace(src['origins'], src['directions'], cap=job.cap, threads=4)
+        ro = O.readout(src, ref, job.cap)
+        assert got['ehss_angstrom2'] == pytest.approx(ro['ehss_angstrom2'], rel=CCS_RTOL)
+        assert got['tail_bound_angstrom2'] == pytest.approx(ro['tail_bound_angstrom2'], rel=1e-15)
+        assert got['pa_from_same_rays_angstrom2'] == pytest.approx(ro['pa_from_same_rays_angstrom2'], rel=1e-15)
+        assert got['unresolved_rays'] == ro['unresolved_rays']
+        assert got['collision_histogram'] == ro['collision_histogram']
+        np.testing.assert_allclose(got['collision_contribution_angstrom2'], ro['collision_contribution_angstrom2'],
+                                   rtol=1e-10, atol=1e-12)
+        hits, _, _ = pat.query(src['origins'], src['directions'], threads=4)
+        assert got['pa_blocked_rays'] == int(hits.sum())
+
+
+def test_blocks_same_alone_and_in_a_mix(eb):
+    from ehss_b200 import workloads as W
+    from ehss_b200.blocks import BlockJob, BlockPlan
+    scenes = [eb.Scene(*W.globule(n, n)[:2]) for n in (20, 300, 1200)]
+    alone = []
+    for sc in scenes:
+        p = BlockPlan([BlockJob(sc, 12, 77, tag=sc.n_atoms)])
+        p.run()
+        alone.append(p.collect()[0])
+    mix = BlockPlan([BlockJob(sc, 12, 77, tag=sc.n_atoms) for sc in scenes[::-1]]
+                    + [BlockJob(scenes[0], 14, 5, tag='extra')], launch=dict(chunk_rays=64, ctas_per_sm=2))
+    mix.run()
+    got = {r['tag']: r for r in mix.collect()}
+    for a in alone:
+        b = got[a['tag']]
+        for key in ('ehss_angstrom2', 'tail_bound_angstrom2', 'pa_from_same_rays_angstrom2', 'collision_histogram',
+                    'collision_contribution_angstrom2'):
+            assert a[key] == b[key], key
+
+
+def test_blocks_cuda_graph_replay(eb):
+    from ehss_b200 import workloads as W
+    from ehss_b200.blocks import BlockJob, BlockPlan
+    sc = eb.Scene(*W.globule(400, 2)[:2])
+    plan = BlockPlan([BlockJob(sc, 13, s) for s in (1, 2, 3)])
+    plan.run()
+    first = plan.collect()
+    plan.capture()
+    for _ in range(3):
+        plan.run()
+    again = plan.collect()
+    assert [r['ehss_angstrom2'] for r in first] == [r['ehss_angstrom2'] for r in again]
+
+
+@pytest.mark.parametrize('name', ['cloud37', 'cloud300', 'tri'])
+def test_pa_anyhit_bit_exact(eb, golden, name):
+    from ehss_b200.state import EHSSSource
+    g = golden('pa.npz')
+    s = eb.Spheres(g[name + '_centers'], g[name + '_radii'], deduplicate=False)
+    idx = eb.SphereIndex(s)
+    n = len(g[name + '_weights'])
+    src = EHSSSource(g[name + '_origins'], g[name + '_directions'], g[name + '_directions'], g[name + '_weights'],
+                     np.full(n, -1), np.zeros(n, dtype=np.int64), 'fixture')
+    hits, boxes, tests = idx.query(src)
+    np.testing.assert_array_equal(hits, g[name + '_hits'])
+    assert tests > 0
+
+
+def test_known_answers(eb):
+    from ehss_b200 import EHSSSource, Spheres
+    # single sphere: omega ~ pi r^2, every ray bounces once (test_ehss_reference.py:9-17)
+    for radius in (.01, 1., 100.):
+        s = Spheres(np.array([[2., -1., 4.]]), np.array([radius]))
+        prep = eb.PreparedStaticGPUEHSS(s)
+        src = eb.external_source(s, 14, 98, scene=prep.scene)
+        r = prep.engine.trace(src, 4)
+        assert r.escaped.all() and not r.unresolved.any() and np.all(r.bounces == 1)
+        assert r.omega == pytest.approx(np.pi * radius * radius, rel=1e-6)
+        assert r.pa == pytest.approx(np.pi * radius * radius, rel=1e-7)
+        assert np.allclose(np.linalg.norm(r.outgoing, axis=1), 1., atol=1e-14)
+    # trapped two-sphere path (test_ehss_reference.py:37-44)
+    s = Spheres(np.array([[-2., 0., 0.], [2., 0., 0.]]), np.ones(2))
+    one = np.array([[1., 0., 0.]])
+    for precision in ('fp64', 'fp32'):
+        r = eb.PreparedStaticGPUEHSS(s, precision=precision).engine.trace(
+            EHSSSource(np.zeros((1, 3)), one, one, np.ones(1), np.array([-1]), np.array([0]), 'diag'), 7, True)
+        assert r.unresolved[0] and not r.escaped[0]
+        assert r.collider_ids[0].tolist() == [1, 0, 1, 0, 1, 0, 1]
+        assert r.omega == 0 and r.tail_bound == 2.
+    # small positive gap is not skipped (test_ehss_reference.py:69-73)
+    gap = 1e-10
+    s = Spheres(np.array([[0., 0., 0.], [2. + gap, 0., 0.]]), np.ones(2))
+    for precision in ('fp64', 'fp32'):
+        r = eb.PreparedStaticGPUEHSS(s, precision=precision).engine.trace(
+            EHSSSource(np.array([[1., 0., 0.]]), one, one, np.ones(1), np.array([0]), np.array([1]), 'gap'), 3, True)
+        assert r.collider_ids[0].tolist()[:2] == [0, 1]
+
+
+def test_empty_and_far_origins(eb):
+    from ehss_b200 import EHSSSource, Spheres
+    s = Spheres(np.array([[-2., 0., 0.], [2., 0., 0.]]), np.ones(2))
+    eng = eb.PreparedStaticGPUEHSS(s).engine
+    empty = EHSSSource(np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 3)), np.ones(0), np.full(0, -1),
+                       np.zeros(0, dtype=int), 'empty')
+    r = eng.trace(empty, 7, True)
+    assert r.positions.shape == (0, 3) and r.tail_bound == 0
+    # an origin far outside the structure takes the FP64 all-atom search
+    o = np.array([[-1000., 0.3, 0.]]); d = np.array([[1., 0., 0.]])
+    src = EHSSSource(o, d, d, np.ones(1), np.array([-1]), np.array([0]), 'far')
+    got = eng.trace(src, 8, True)
+    t = O.StaticTree(s.centers, s.radii, 4)
+    ref = t.trace(o, d, cap=8, record=True)
+    np.testing.assert_array_equal(got.outgoing, ref['outgoing'])
+    np.testing.assert_array_equal(got.collider_ids, ref['collider_ids'])
+
+
+def test_comoving_rotation_and_permutation_invariance(eb):
+    """test_ehss_publication_invariance.py:14-43 on the device."""
+    from ehss_b200 import EHSSSource, Spheres
+    s = Spheres(np.array([[0., 0., 0.], [4., 0., 0.], [1., 5., 0.], [.5, 1., 6.]]), np.full(4, 3.1),
+                deduplicate=False)
+    src = eb.external_source(s, 12, 170100001)
+    base = eb.PreparedStaticGPUEHSS(s).engine.trace(src, 256, True)
+    order = np.array([3, 1, 0, 2])
+    moved = Spheres(s.centers[order], s.radii[order], deduplicate=False)
+    perm = eb.PreparedStaticGPUEHSS(moved).engine.trace(src, 256, True)
+    np.testing.assert_array_equal(perm.outgoing, base.outgoing)
+    mapped = perm.collider_ids.copy(); valid = mapped >= 0; mapped[valid] = order[mapped[valid]]
+    np.testing.assert_array_equal(mapped, base.collider_ids)
+    from ehss_b200.workloads import random_rotation
+    rot = random_rotation(3)
+    for scale in (.01, 1., 100.):
+        shift = scale * np.array([9., -4., 7.])
+        ms = Spheres(scale * s.centers @ rot.T + shift, scale * s.radii, deduplicate=False)
+        rays = EHSSSource(scale * src.origins @ rot.T + shift, src.directions @ rot.T, src.incoming @ rot.T,
+                          src.weights * scale ** 2, src.last_atom.copy(), src.initial_bounces.copy(), 'co-moving')
+        r = eb.PreparedStaticGPUEHSS(ms).engine.trace(rays, 256, True)
+        np.testing.assert_array_equal(r.escaped, base.escaped)
+        np.testing.assert_array_equal(r.bounces, base.bounces)
+        np.testing.assert_array_equal(r.collider_ids, base.collider_ids)
+        assert r.omega / scale ** 2 == pytest.approx(base.omega, rel=1e-9)
+
+
+def test_invalid_inputs_raise(eb):
+    from ehss_b200 import EHSSSource, Spheres
+    s = Spheres(np.array([[0., 0., 0.]]), np.ones(1))
+    eng = eb.PreparedStaticGPUEHSS(s).engine
+    one = np.array([[1., 0., 0.]])
+    src = EHSSSource(np.array([[-3., 0., 0.]]), one, one, np.ones(1), np.array([-1]), np.array([0]), 'x')
+    with pytest.raises(ValueError):
+        eng.trace(src, 0)
+    bad = EHSSSource(np.array([[-3., 0., 0.]]), one, one, np.ones(1), np.array([5]), np.array([1]), 'x')
+    with pytest.raises(ValueError):
+        eng.trace(bad, 4)
+    with pytest.raises(ValueError):
+        eb.PreparedStaticGPUEHSS(Spheres([[0, 0, 0], [2, 0, 0]], [1, 1]), groups=[0, 2])

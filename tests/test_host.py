@@ -1,0 +1,128 @@
+"""Host-side logic that needs no GPU: the C ABI loads and exports what the
+header declares, the host Sobol scrambler is bit-exact, block preparation,
+argument validation, workload generators and the reference data types."""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+@pytest.fixture(scope='module')
+def lib():
+    from ehss_b200 import _lib
+    return _lib.load()
+
+
+def test_library_exports_every_header_function(lib):
+    from ehss_b200 import _lib
+    declared = _lib.header_functions()
+    assert len(declared) >= 15
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(declared) == set(_lib._SIGNATURES), 'ctypes table and header differ'
+    assert lib.ehss_abi_version() == 1
+
+
+@pytest.mark.parametrize('dim', [1, 2, 4, 5, 8])
+def test_host_sobol_scramble_bit_exact(lib, dim):
+    for seed in (0, 1, 98, 190003, 2 ** 32 - 1, 2 ** 40 + 5, 2 ** 64 - 1):
+        sv = (ct.c_uint32 * (dim * 30))(); sh = (ct.c_uint32 * dim)()
+        assert lib.ehss_sobol_scramble(dim, seed, sv, sh) == 0
+        ref_sv, ref_sh = O.sobol_scramble(dim, seed)
+        np.testing.assert_array_equal(np.array(sv[:]).reshape(dim, 30), ref_sv)
+        np.testing.assert_array_equal(np.array(sh[:]), ref_sh)
+
+
+def test_host_sobol_against_golden_scrambles(lib, golden):
+    g = golden('sobol.npz')
+    for key in sorted({k.rsplit('_', 1)[0] for k in g if k.startswith('d')}):
+        d, m, s = (int(part[1:]) for part in key.split('_'))
+        sv = (ct.c_uint32 * (d * 30))(); sh = (ct.c_uint32 * d)()
+        assert lib.ehss_sobol_scramble(d, s, sv, sh) == 0
+        np.testing.assert_array_equal(np.array(sv[:]).reshape(d, 30), g[key + '_sv'])
+        np.testing.assert_array_equal(np.array(sh[:]), g[key + '_shift'])
+
+
+def test_argument_validation_without_device(lib):
+    from ehss_b200 import _lib
+    sb, wb = ct.c_uint64(), ct.c_uint64()
+    assert lib.ehss_scene_bytes(0, 4, ct.byref(sb), ct.byref(wb)) == _lib.ERR_VALUE
+    assert b'atom count' in lib.ehss_last_error()
+    assert lib.ehss_scene_bytes(10, 9, ct.byref(sb), ct.byref(wb)) == _lib.ERR_VALUE
+    assert lib.ehss_scene_bytes(1000, 4, ct.byref(sb), ct.byref(wb)) == 0
+    assert sb.value % 256 == 0 and sb.value >= 256 + 999 * 64 + 1000 * (16 + 32 + 8)
+    sv = (ct.c_uint32 * 300)(); sh = (ct.c_uint32 * 10)()
+    assert lib.ehss_sobol_scramble(9, 0, sv, sh) == _lib.ERR_VALUE
+    assert lib.ehss_trace(None, 1, 0, 1, *([None] * 8), None) == _lib.ERR_VALUE
+    with pytest.raises(ValueError):
+        _lib.check(_lib.ERR_VALUE)
+
+
+def test_blocks_prepare_chunks_and_offsets(lib):
+    from ehss_b200 import _lib
+    n = 3
+    blocks = (_lib.Block * n)()
+    for i, (log2, cap) in enumerate([(12, 64), (5, 1), (14, 7)]):
+        blocks[i].scene = 0x1000 * (i + 1)
+        blocks[i].log2_rays = log2
+        blocks[i].cap = cap
+        blocks[i].precision = 1
+        blocks[i].flags = _lib.BLOCK_EHSS
+        blocks[i].hist_offset = -1
+    seeds = (ct.c_uint64 * n)(0, 1, 2)
+    total = ct.c_int64()
+    assert lib.ehss_blocks_prepare(blocks, n, seeds, 256, ct.byref(total)) == 0
+    assert total.value == 16 + 1 + 64
+    assert [b.chunk_begin for b in blocks] == [0, 16, 17]
+    assert [b.hist_offset for b in blocks] == [0, 65, 67]
+    sv, sh = O.sobol_scramble(4, 2)
+    np.testing.assert_array_equal(np.array([[blocks[2].sv[k][j] for j in range(4)] for k in range(30)]), sv.T)
+    np.testing.assert_array_equal(np.array(blocks[2].shift[:]), sh)
+    blocks[1].cap = 0
+    assert lib.ehss_blocks_prepare(blocks, n, seeds, 256, ct.byref(total)) == _lib.ERR_VALUE
+    assert lib.ehss_blocks_prepare(blocks, n, seeds, 100, ct.byref(total)) == _lib.ERR_VALUE
+
+
+def test_struct_layouts_match_header():
+    from ehss_b200 import _lib
+    assert ct.sizeof(_lib.Block) == 8 + 480 + 16 + 16 + 16
+    assert ct.sizeof(_lib.BlockResult) == 8 * (5 + _lib.NSTATS)
+    assert ct.sizeof(_lib.Launch) == 16
+
+
+def test_workload_generators():
+    from ehss_b200 import workloads as W
+    from scipy.spatial import cKDTree
+    c, r, e = W.globule(650, 4)
+    assert c.shape == (650, 3) and len(e) == 650
+    assert cKDTree(c).query(c, k=2)[0][:, 1].min() >= 1.0 - 1e-12
+    c2, _, _ = W.globule(650, 4)
+    np.testing.assert_array_equal(c, c2)
+    set_r = set(np.round(r, 6))
+    assert set_r <= {round(W.VDW_RADII[x] + 1.4, 6) for x in W.ELEMENTS}
+    batch = W.mixed_batch(256, seed=1)
+    ns = np.array([b[0] for b in batch]); logs = np.array([b[1] for b in batch])
+    assert ns.min() >= 20 and ns.max() <= 5000 and set(logs) <= set(range(14, 19))
+    R = W.random_rotation(5)
+    np.testing.assert_allclose(R @ R.T, np.eye(3), atol=1e-12)
+    assert np.linalg.det(R) == pytest.approx(1.0)
+    xyz, rad, el = W.triatomic()
+    assert np.linalg.norm(xyz[1] - xyz[0]) == pytest.approx(0.9572)
+    assert list(rad) == [2.92, 2.5, 2.5]
+
+
+def test_state_types_validate_like_reference():
+    from ehss_b200 import EHSSSource, Spheres
+    with pytest.raises(ValueError):
+        Spheres(np.zeros((0, 3)), np.zeros(0))
+    with pytest.raises(ValueError):
+        Spheres(np.zeros((1, 3)), np.array([-1.]))
+    s = Spheres(np.array([[0., 0, 0], [0., 0, 0]]), np.ones(2))
+    assert len(s.radii) == 1
+    d = np.array([[1., 0, 0]])
+    with pytest.raises(ValueError):
+        EHSSSource(np.zeros((1, 3)), 2 * d, d, np.ones(1), np.array([-1]), np.array([0]), 'x')
+    with pytest.raises(ValueError):
+        EHSSSource(np.zeros((1, 3)), d, d, np.ones(1), np.array([-1]), np.array([1]), 'x')
