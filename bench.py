@@ -1,0 +1,426 @@
+"""Benchmark of the batched EHSS cross-section path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload batched|plain]
+
+Workload (default, "batched"): 256 synthetic RSA globules (0.1 atoms/A^3,
+1.0 A minimum pair distance, H/C/N/O/S 0.49/0.32/0.09/0.09/0.01) with atom
+counts log-uniform in 20..5000 and ray budgets 2^14..2^18 (log-uniform,
+rounded to powers of two), 3 scrambled-Sobol replicate blocks each, collision
+cap 64, FP32 traversal with FP64 re-test (outcomes identical to FP64).  One
+step = batched LBVH build of all 256 structures + all 768 blocks traced and
+reduced in one persistent launch (CUDA-graph replay).  Inputs (atoms) are
+resident in HBM for `value`; `e2e` runs the public BatchCCS API from pinned
+host arrays to host results.  L2 (126 MB) is flushed by a 256 MB write
+between timed steps.  Metric: EHSS rays/s (whole job); structures/s, the
+plain one-structure-per-launch path, p50/p99 per-structure latency of the
+plain path and the CCS error against the FP64 oracle are reported beside it.
+
+Under torchrun (N > 1) every rank runs its own batch (rank-seeded): weak
+scaling with no data-path collective; the max time over ranks is used.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "EHSS rays/s and structures/s at <=1e-5 rel CCS err; batched vs plain; p50/p99 latency"
+UNIT = "rays/s"
+N_STRUCT = 256
+REPEATS = 3
+CAP = 64
+MASTER_SEED = 2026
+# per-ray FP32 op counts of the reference's sphere and box tests
+# (entry_scalar, ehss_cpu.py:12-24: 35 ops; box_interval, ehss_support_tree.py:20-31: 27 ops)
+C_SPHERE, C_BOX = 35, 27
+CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
+    ap.add_argument('--workload', choices=['batched'], default='batched')
+    ap.add_argument('--structures', type=int, default=N_STRUCT)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-plain', action='store_true')
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    return world, rank, local
+
+
+def make_structures(count, seed):
+    from ehss_b200 import workloads as W
+    spec = W.mixed_batch(count, seed=seed)
+    structures, log2s, seeds = [], [], []
+    for n, lg, s in spec:
+        c, r, _ = W.globule(n, s)
+        structures.append((c, r))
+        log2s.append(lg)
+        seeds.append(s % (2 ** 32))
+    return structures, log2s, seeds
+
+
+def config(args, world):
+    return {"workload": f"batched mixed-size globules: {args.structures} structures/GPU, atoms log-uniform 20..5000, "
+                        f"rays 2^14..2^18 per replicate, {REPEATS} replicates, cap {CAP}",
+            "structures_per_gpu": args.structures, "replicates": REPEATS, "cap": CAP,
+            "precision": "fp32 traversal + fp64 re-test", "master_seed": MASTER_SEED,
+            "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world} (weak)"}
+
+
+# ----------------------------------------------------------------------------
+# clocks
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, index):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--query-gpu={CLOCK_FIELDS}', '--format=csv,noheader,nounits',
+                                          '-lms', '200', '-i', str(index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith('active'):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# oracle-side measurements (CPU): reference op counts, CPU baseline, CCS error
+# ----------------------------------------------------------------------------
+def reference_ops_per_ray(structures, sample_log2=10, seed=12345):
+    """Mean reference sphere/box tests per ray for each structure (oracle counters)."""
+    from oracle import oracle as O
+    ops, s_mean, b_mean = [], [], []
+    for c, r in structures:
+        src = O.external_source(c, r, sample_log2, seed)
+        t = O.StaticTree(c, r, 4)
+        res = t.trace(src['origins'], src['directions'], cap=CAP, threads=O.host_cores())
+        n = len(src['origins'])
+        s, b = res['sphere_tests'] / n, res['box_tests'] / n
+        s_mean.append(s); b_mean.append(b)
+        ops.append(C_SPHERE * s + C_BOX * b)
+    return np.array(ops), np.array(s_mean), np.array(b_mean)
+
+
+def cpu_reference_rate(structures, log2, seed, budget_s=12.0, threads=None):
+    """Rays/s of the reference's own C++ kernel (oracle/_ref) on a bounded sample."""
+    from oracle import oracle as O
+    threads = threads or O.host_cores()
+    kind = 'reference' if O.ref_available() else 'port'
+    prepared = []
+    for c, r in structures:
+        src = O.external_source(c, r, log2, seed)
+        prepared.append((O.StaticTree(c, r, 4), src['origins'], src['directions']))
+    rays, elapsed, passes = 0, 0.0, 0
+    while elapsed < budget_s or passes == 0:
+        t0 = time.perf_counter()
+        for tree, o, d in prepared:
+            if kind == 'reference':
+                O.ref_trace(tree, o, d, cap=CAP, threads=threads)
+            else:
+                tree.trace(o, d, cap=CAP, threads=threads)
+            rays += len(o)
+        elapsed += time.perf_counter() - t0
+        passes += 1
+    return rays / elapsed, kind, threads, rays, elapsed
+
+
+def ccs_error_vs_oracle(eb, structures, log2=12, seed=777):
+    """Max relative CCS error of the FP32 device path vs the FP64 oracle on the same rays."""
+    from oracle import oracle as O
+    from ehss_b200.blocks import BlockJob, BlockPlan
+    worst = 0.0
+    for c, r in structures:
+        scene = eb.Scene(c, r)
+        plan = BlockPlan([BlockJob(scene, log2, seed, cap=CAP)])
+        plan.run()
+        got = plan.collect()[0]['ehss_angstrom2']
+        o, d = scene.source_rays(log2, seed)
+        o, d = o.cpu().numpy(), d.cpu().numpy()
+        res = O.StaticTree(c, r, 4).trace(o, d, cap=CAP, threads=O.host_cores())
+        n = len(o)
+        ro = O.readout(dict(incoming=d, weights=np.full(n, np.pi * scene.radius ** 2 / n)), res, CAP)
+        worst = max(worst, abs(got - ro['ehss_angstrom2']) / ro['ehss_angstrom2'])
+    return worst
+
+
+def peaks():
+    p = ROOT / 'MEASURED_PEAKS.json'
+    try:
+        return json.loads(p.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def traffic_per_launch():
+    p = ROOT / 'profiles' / 'k_blocks_traffic.json'
+    try:
+        return json.loads(p.read_text())
+    except (OSError, ValueError):
+        return None
+
+
+# ----------------------------------------------------------------------------
+# reference arm
+# ----------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    structures, log2s, seeds = make_structures(args.structures, MASTER_SEED)
+    sample = structures[::8]
+    threads = O.host_cores()
+    kind = 'reference' if O.ref_available() else 'port'
+    prepared = []
+    for c, r in sample:
+        src = O.external_source(c, r, 12, 190003)
+        prepared.append((O.StaticTree(c, r, 4), src['origins'], src['directions']))
+    rays_step = sum(len(o) for _, o, _ in prepared)
+
+    def step():
+        for tree, o, d in prepared:
+            if kind == 'reference':
+                O.ref_trace(tree, o, d, cap=CAP, threads=threads)
+            else:
+                tree.trace(o, d, cap=CAP, threads=threads)
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = rays_step * args.steps / dt
+    sample_txt = f"{len(sample)} of {len(structures)} structures (every 8th), 2^12 rays each, cap {CAP}, per step"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config(args, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample_txt},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+def main():
+    args = parse()
+    world, rank, local = dist_env()
+    if args.impl == 'reference':
+        run_reference(args, world, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    if not torch.cuda.is_available():
+        raise SystemExit('bench.py needs a CUDA device')
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=600), device_id=torch.device('cuda', local))
+    import ehss_b200 as eb
+    from ehss_b200 import _lib
+    from ehss_b200.batch import BatchCCS
+    from ehss_b200.blocks import BlockPlan
+    _lib.load()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    structures, log2s, seeds = make_structures(args.structures, MASTER_SEED + rank)
+    bc = BatchCCS(structures, log2s, seeds, repeats=REPEATS, cap=CAP, precision='fp32')
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+    stream = torch.cuda.current_stream()
+
+    bc.upload()
+    for _ in range(max(args.warmup, 3)):
+        bc.build()
+        bc.trace()
+    torch.cuda.synchronize()
+
+    # -- device-resident steps ---------------------------------------------------
+    step_ms, trace_ms = [], []
+    barrier(); torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        bc.build()
+        e1.record(stream)
+        bc.trace()
+        e2.record(stream)
+        e2.synchronize()
+        step_ms.append(e0.elapsed_time(e2)); trace_ms.append(e1.elapsed_time(e2))
+    torch.cuda.synchronize(); barrier()
+    clocks = sampler.stop()
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device='cuda', dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    rays_step = bc.rays
+    value = rays_step * world * args.steps / (total_ms * 1e-3)
+    structs_per_s = args.structures * world * args.steps / (total_ms * 1e-3)
+    mean_trace_ms = float(np.mean(trace_ms))
+    stats = np.sum([r['stats'] for r in bc.plan.collect()], axis=0)
+
+    # -- end to end through the public API (pinned host in, host results out) -----
+    e2e_ms = []
+    for _ in range(max(2, args.steps // 4)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        results = bc.run()
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_total = float(np.mean(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_total], device='cuda', dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = rays_step * world / (e2e_total * 1e-3)
+
+    # -- plain path: one structure per build + launch, no graph --------------------
+    plain = None
+    if not args.no_plain:
+        from ehss_b200.blocks import BlockJob
+        lib = _lib.load()
+        import ctypes as ct
+        plans = []
+        for s, sc in enumerate(bc.scenes):
+            jobs = [j for j in bc.plan.jobs if j.tag[0] == s]
+            plans.append(BlockPlan([BlockJob(j.scene, j.log2_rays, j.seed, cap=j.cap, precision=j.precision,
+                                             tag=j.tag) for j in jobs]))
+        ws = torch.empty(bc.ws_bytes + 256, dtype=torch.uint8, device='cuda')
+        ws_ptr = (ws.data_ptr() + 255) & ~255
+        sh = torch.cuda.current_stream().cuda_stream
+
+        def plain_structure(s):
+            _lib.check(lib.ehss_scene_build(int(bc.n_atoms[s]), bc._xyz_ptrs[s], bc._r_ptrs[s], bc.leaf_size,
+                                            bc.scene_ptrs[s], bc._sizes[s], ws_ptr, bc.ws_bytes, sh))
+            plans[s].enqueue()
+        for s in range(len(plans)):          # warm-up
+            plain_structure(s)
+        torch.cuda.synchronize()
+        lat = []
+        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        t0.record(stream)
+        for s in range(len(plans)):
+            a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            plain_structure(s)
+            b.record(stream)
+            lat.append((a, b))
+        t1.record(stream)
+        t1.synchronize()
+        plain_ms = t0.elapsed_time(t1)
+        lats = np.array([a.elapsed_time(b) for a, b in lat])
+        plain = {"rays_per_s": rays_step / (plain_ms * 1e-3), "structures_per_s": args.structures / (plain_ms * 1e-3),
+                 "ms_per_pass": plain_ms, "latency_ms_p50": float(np.percentile(lats, 50)),
+                 "latency_ms_p99": float(np.percentile(lats, 99))}
+
+    # -- roofline, CPU baseline and CCS error (rank 0, N = 1 only for the baseline) ---
+    pk = peaks()
+    sm_max = float(pk.get('sm_max_mhz', 1965.0))
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    peak_tflops = n_sm * 128 * 2 * sm_max * 1e6 / 1e12
+    roof = None
+    cpu = None
+    ccs_err = None
+    if rank == 0:
+        ops, s_ref, b_ref = reference_ops_per_ray(structures)
+        ray_counts = np.array([(1 << lg) * REPEATS for lg in log2s], dtype=np.float64)
+        ops_step = float(np.sum(ray_counts * ops))
+        achieved = ops_step / (mean_trace_ms * 1e-3) / 1e12
+        traffic = traffic_per_launch()
+        roof = {"bound": "fp32", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+                "frac": achieved / peak_tflops,
+                "traffic": traffic.get('bytes_per_launch') if traffic else None,
+                "kernel": "ehss::k_blocks", "kernel_ms": mean_trace_ms,
+                "ops_per_ray": ops_step / rays_step,
+                "ref_sphere_tests_per_ray": float(np.sum(ray_counts * s_ref) / ray_counts.sum()),
+                "ref_box_tests_per_ray": float(np.sum(ray_counts * b_ref) / ray_counts.sum()),
+                "peak_note": f"nominal FP32: {n_sm} SMs x 128 lanes x 2 x {sm_max:.0f} MHz (no measured FP32 peak)"}
+        ccs_err = ccs_error_vs_oracle(eb, structures[::32])
+        if world == 1 and not args.no_cpu_baseline:
+            rate, kind, cores, rays_done, secs = cpu_reference_rate(structures[::16], 12, 190003)
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                   "sample": f"{len(structures[::16])} of {len(structures)} structures (every 16th), 2^12 rays each, "
+                             f"cap {CAP}; {rays_done} rays in {secs:.1f} s"}
+    if rank == 0:
+        launches_per_step = 8   # 7 LBVH builder kernels + 1 persistent trace kernel (CUB sort kernels not counted)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+                "config": config(args, world),
+                "structures_per_s": structs_per_s,
+                "rays_per_step": rays_step * world,
+                "trace_ms_per_step": mean_trace_ms, "build_ms_per_step": float(np.mean(step_ms) - mean_trace_ms),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bc.h2d_bytes,
+                        "d2h_bytes_per_step": bc.d2h_bytes, "ms_per_step": e2e_total,
+                        "structures_per_s": args.structures * world / (e2e_total * 1e-3)},
+                "plain": plain,
+                "batched_over_plain": (value / world / plain['rays_per_s']) if plain else None,
+                "ccs_rel_err_max_vs_fp64_oracle": ccs_err,
+                "grazing_queries": int(stats[_lib.STAT_GRAZING]), "fp64_fallback_queries": int(stats[_lib.STAT_FALLBACK]),
+                "queries": int(stats[_lib.STAT_QUERIES]),
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+                "gpu_launches": launches_per_step * args.steps}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

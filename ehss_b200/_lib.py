@@ -33,9 +33,9 @@ class SceneInfo(ct.Structure):
 
 
 class Block(ct.Structure):
-    _fields_ = [('scene', P), ('sv', (ct.c_uint32 * 4) * 30), ('shift', ct.c_uint32 * 4), ('log2_rays', I32),
+    _fields_ = [('sv', (ct.c_uint32 * 4) * 30), ('shift', ct.c_uint32 * 4), ('scene', P), ('log2_rays', I32),
                 ('cap', I32), ('precision', I32), ('flags', ct.c_uint32), ('hist_offset', I64),
-                ('chunk_begin', I64)]
+                ('chunk_begin', I64), ('reserved', I64)]
 
 
 class BlockResult(ct.Structure):

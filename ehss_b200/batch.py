@@ -1,0 +1,143 @@
+"""Batched cross sections: many structures, one build pass, one persistent launch.
+
+``BatchCCS`` is the public entry for the batched form: it takes host arrays
+of many structures of uneven size, stages them in pinned memory, builds every
+LBVH in one pass of the builder kernels (ehss_scenes_build), runs all
+(structure, replicate) blocks in one persistent launch (optionally replayed
+from a CUDA graph) and returns per-structure EHSS/PA summaries with the
+reference CLI's replicate statistics (ccs_cli.summarize, ccs_cli.py:163-167).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+
+import numpy as np
+
+from . import _lib
+from .blocks import BlockJob, BlockPlan, seed_schedule
+from .device import require_cuda, stream_handle, torch
+
+
+def enclosing_radius(centers, radii):
+    """Impact-disk radius exactly as the device computes it (ehss_state.py:46-47)."""
+    center = centers.mean(axis=0)
+    return float(np.max(np.linalg.norm(centers - center, axis=1) + radii)) * (1. + 1e-9)
+
+
+def summarize(values):
+    a = np.asarray(values, dtype=float)
+    sd = float(a.std(ddof=1)) if len(a) > 1 else None
+    return dict(mean=float(a.mean()), sd=sd, sem=sd / math.sqrt(len(a)) if sd is not None else None,
+                replicates=len(a))
+
+
+class SceneRef:
+    """A scene inside a batch buffer (what BlockPlan needs of a scene)."""
+
+    def __init__(self, ptr, radius, n_atoms, device):
+        self.ptr, self.radius, self.n_atoms, self.device = ptr, radius, n_atoms, device
+
+
+class BatchCCS:
+    def __init__(self, structures, log2_rays, seeds, repeats=3, cap=64, precision='fp32', ehss=True, pa=False,
+                 leaf_size=4, launch=None, device=None, graph=True):
+        lib = _lib.load()
+        t = torch()
+        self.device = require_cuda(device)
+        S = len(structures)
+        if S < 1:
+            raise ValueError('at least one structure required')
+        log2s = [int(log2_rays)] * S if np.isscalar(log2_rays) else [int(x) for x in log2_rays]
+        seeds = [int(x) for x in (seeds if not np.isscalar(seeds) else [seeds] * S)]
+        self.n_atoms = np.array([len(r) for _, r in structures], dtype=np.int64)
+        if np.any(self.n_atoms < 1):
+            raise ValueError('every structure needs at least one atom')
+        N = int(self.n_atoms.sum())
+        self.atom0 = np.concatenate([[0], np.cumsum(self.n_atoms)[:-1]])
+        # pinned host staging, one contiguous copy per array
+        self.h_xyz = t.empty(N * 3, dtype=t.float64, pin_memory=True)
+        self.h_r = t.empty(N, dtype=t.float64, pin_memory=True)
+        hx, hr = self.h_xyz.numpy(), self.h_r.numpy()
+        radii = []
+        for (c, r), a0, n in zip(structures, self.atom0, self.n_atoms):
+            c = np.ascontiguousarray(c, dtype=np.float64); r = np.ascontiguousarray(r, dtype=np.float64)
+            if c.shape != (n, 3) or not np.isfinite(c).all() or not np.isfinite(r).all() or np.any(r <= 0):
+                raise ValueError('Finite centers (N,3) and positive finite radii required.')
+            hx[3 * a0:3 * (a0 + n)] = c.ravel()
+            hr[a0:a0 + n] = r
+            radii.append(enclosing_radius(c, r))
+        self.d_xyz = t.empty(N * 3, dtype=t.float64, device=self.device)
+        self.d_r = t.empty(N, dtype=t.float64, device=self.device)
+        # scene buffers carved from one allocation
+        sizes = []
+        for n in self.n_atoms:
+            sb, wb = ct.c_uint64(), ct.c_uint64()
+            _lib.check(lib.ehss_scene_bytes(int(n), int(leaf_size), ct.byref(sb), ct.byref(wb)), 'scene size')
+            sizes.append(sb.value)
+        offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        self.scene_buf = t.empty(int(sum(sizes)) + 256, dtype=t.uint8, device=self.device)
+        base = (self.scene_buf.data_ptr() + 255) & ~255
+        self.scene_ptrs = [base + int(o) for o in offs]
+        wb = ct.c_uint64()
+        _lib.check(lib.ehss_scenes_workspace_bytes(S, (ct.c_int64 * S)(*self.n_atoms), ct.byref(wb)), 'workspace')
+        self.ws = t.empty(int(wb.value) + 256, dtype=t.uint8, device=self.device)
+        self.ws_ptr = (self.ws.data_ptr() + 255) & ~255
+        self.ws_bytes = int(wb.value)
+        xp = self.d_xyz.data_ptr(); rp = self.d_r.data_ptr()
+        self._xyz_ptrs = (ct.c_void_p * S)(*[xp + 24 * int(a) for a in self.atom0])
+        self._r_ptrs = (ct.c_void_p * S)(*[rp + 8 * int(a) for a in self.atom0])
+        self._n = (ct.c_int64 * S)(*self.n_atoms)
+        self._scenes = (ct.c_void_p * S)(*self.scene_ptrs)
+        self._sizes = (ct.c_uint64 * S)(*sizes)
+        self.leaf_size = int(leaf_size)
+        self.scenes = [SceneRef(p, R, int(n), self.device) for p, R, n in zip(self.scene_ptrs, radii, self.n_atoms)]
+        prec = {'fp64': _lib.PREC_FP64, 'fp32': _lib.PREC_FP32}[precision] if isinstance(precision, str) else precision
+        jobs = []
+        for s, (sc, lg, sd) in enumerate(zip(self.scenes, log2s, seeds)):
+            for k, seed in enumerate(seed_schedule(sd, repeats)):
+                jobs.append(BlockJob(sc, lg, seed, cap=cap, precision=prec, ehss=ehss, pa=pa, tag=(s, k)))
+        self.repeats = int(repeats)
+        self.plan = BlockPlan(jobs, launch=launch, device=self.device)
+        self.rays = self.plan.rays
+        self.use_graph = graph
+        self.h2d_bytes = (N * 3 + N) * 8
+        self.d2h_bytes = self.plan.results.numel() + 16 * self.plan.hist.numel()
+
+    # -- stages ---------------------------------------------------------------
+    def upload(self):
+        self.d_xyz.copy_(self.h_xyz, non_blocking=True)
+        self.d_r.copy_(self.h_r, non_blocking=True)
+
+    def build(self):
+        lib = _lib.load()
+        _lib.check(lib.ehss_scenes_build(len(self.scenes), self._xyz_ptrs, self._r_ptrs, self._n, self.leaf_size,
+                                         self._scenes, self._sizes, self.ws_ptr, self.ws_bytes,
+                                         stream_handle(self.device)), 'batched scene build')
+
+    def trace(self):
+        if self.use_graph and self.plan.graph is None:
+            self.plan.capture()
+        self.plan.run()
+
+    def download(self):
+        blocks = self.plan.collect()
+        out = [dict(structure=s, atoms=sc.n_atoms, runs=[]) for s, sc in enumerate(self.scenes)]
+        for b in blocks:
+            out[b['tag'][0]]['runs'].append(b)
+        for o in out:
+            runs = o['runs']
+            if 'ehss_angstrom2' in runs[0]:
+                o['ehss_angstrom2'] = summarize([r['ehss_angstrom2'] for r in runs])
+                o['ehss_tail_bound_mean_angstrom2'] = float(np.mean([r['tail_bound_angstrom2'] for r in runs]))
+                o['ehss_unresolved_rays_total'] = int(sum(r['unresolved_rays'] for r in runs))
+            if 'pa_angstrom2' in runs[0]:
+                o['pa_angstrom2'] = summarize([r['pa_angstrom2'] for r in runs])
+        return out
+
+    def run(self):
+        """Host arrays in, per-structure results out (upload, build, trace, download)."""
+        self.upload()
+        self.build()
+        self.trace()
+        return self.download()

@@ -4,6 +4,7 @@
 #include <math_constants.h>
 #include <cstdint>
 #include <cfloat>
+#include <cstddef>
 #include "../../include/ehss_b200.h"
 
 namespace ehss {
@@ -50,6 +51,8 @@ struct alignas(256) SceneHeader {
     uint64_t bytes;
 };
 static_assert(sizeof(SceneHeader) == 256, "scene header is one 256-byte line");
+static_assert(sizeof(ehss_block) % 16 == 0 && offsetof(ehss_block, sv) == 0 && offsetof(ehss_block, shift) == 480,
+              "block descriptors are read with 16-byte vector loads");
 
 struct SceneView {
     const SceneHeader* h;

@@ -474,11 +474,10 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
                              "scene header upload");
         if (rc) { delete[] host; return rc; }
     }
+    // A copy from pageable host memory has staged its source when the call
+    // returns, so the host descriptors (and the headers above) may go now.
     int rc = cuda_status(cudaMemcpyAsync(W.descs, host, sizeof(BuildDesc) * S, cudaMemcpyHostToDevice, stream),
                          "build descriptor upload");
-    if (rc) { delete[] host; return rc; }
-    // pageable copies above are staged before returning, so the host array may go
-    rc = cuda_status(cudaStreamSynchronize(stream), "build descriptor upload");
     delete[] host;
     if (rc) return rc;
 

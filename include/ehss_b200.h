@@ -157,16 +157,19 @@ int ehss_pa_anyhit(const void* scene_dev, int64_t n_rays, const double* origins_
 #define EHSS_BLOCK_EHSS 1u      /* trace EHSS */
 #define EHSS_BLOCK_PA 2u        /* any-hit PA on the same rays */
 
+/* 544 bytes, a multiple of 16: the device reads sv/shift as 16-byte vectors,
+ * so a device array of blocks must start on a 16-byte boundary. */
 typedef struct ehss_block {
+    uint32_t sv[30][4];       /* Sobol(4) direction numbers, [bit][dim] (offset 0) */
+    uint32_t shift[4];        /* offset 480 */
     const void* scene;        /* device scene buffer */
-    uint32_t sv[30][4];       /* Sobol(4) direction numbers, [bit][dim] */
-    uint32_t shift[4];
     int32_t log2_rays;        /* 3..24 */
     int32_t cap;              /* collision cap >= 1 */
     int32_t precision;        /* EHSS_PREC_* */
     uint32_t flags;           /* EHSS_BLOCK_* */
-    int64_t hist_offset;      /* first hist/ledger entry of this block */
+    int64_t hist_offset;      /* first hist/ledger entry of this block (-1: next free) */
     int64_t chunk_begin;      /* filled by ehss_blocks_prepare */
+    int64_t reserved;         /* 0 */
 } ehss_block;
 
 typedef struct ehss_block_result {

@@ -87,7 +87,7 @@ def test_blocks_prepare_chunks_and_offsets(lib):
 
 def test_struct_layouts_match_header():
     from ehss_b200 import _lib
-    assert ct.sizeof(_lib.Block) == 8 + 480 + 16 + 16 + 16
+    assert ct.sizeof(_lib.Block) == 544 and _lib.Block.sv.offset == 0 and _lib.Block.shift.offset == 480
     assert ct.sizeof(_lib.BlockResult) == 8 * (5 + _lib.NSTATS)
     assert ct.sizeof(_lib.Launch) == 16
 
