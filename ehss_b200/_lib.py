@@ -54,6 +54,7 @@ _SIGNATURES = {
     'ehss_sobol_points': (ct.c_int, [ct.c_int, U64, I64, I64, P, P]),
     'ehss_scene_bytes': (ct.c_int, [I64, ct.c_int, P, P]),
     'ehss_scene_build': (ct.c_int, [I64, P, P, ct.c_int, P, U64, P, U64, P]),
+    'ehss_scene_build_noalloc': (ct.c_int, [I64, P, P, ct.c_int, P, U64, P]),
     'ehss_scenes_workspace_bytes': (ct.c_int, [ct.c_int, P, P]),
     'ehss_scenes_build': (ct.c_int, [ct.c_int, P, P, P, ct.c_int, P, P, P, U64, P]),
     'ehss_scene_info_get': (ct.c_int, [P, P, P]),

@@ -96,6 +96,21 @@ int ehss_scene_build(int64_t n_atoms, const double* xyz_dev, const double* radii
                      void* scene_dev, uint64_t scene_bytes, void* workspace_dev, uint64_t workspace_bytes,
                      void* stream);
 
+/* Scene build that allocates nothing.  No counterpart in the reference (its
+ * CPU path never allocates device memory).  For callers that cannot call
+ * cudaMalloc -- a plugin inside a runtime that owns the device's memory pool,
+ * a process under a fixed memory budget -- it builds a scene like
+ * ehss_scene_build but takes the builder's workspace from one fixed 4 MiB
+ * array in device memory declared by the library (held by every GPU that
+ * loads the library until exit).  The caller still passes the inputs and the
+ * scene buffer.  At most EHSS_NOALLOC_MAX_ATOMS atoms (larger: EHSS_ERR_VALUE).
+ * All calls on a device share the array: calls whose work overlaps on the GPU
+ * race, so order them on one stream.  The first call on a device looks up the
+ * array's address; make it before any stream capture. */
+#define EHSS_NOALLOC_MAX_ATOMS 20000
+int ehss_scene_build_noalloc(int64_t n_atoms, const double* xyz_dev, const double* radii_dev, int leaf_size,
+                             void* scene_dev, uint64_t scene_bytes, void* stream);
+
 /* Batched build: n_scenes structures in one pass of the builder kernels
  * (the batched/served forms build every admitted structure at once).
  * Arrays of device pointers and sizes are host arrays of length n_scenes. */
