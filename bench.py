@@ -310,6 +310,14 @@ def main():
     structs_per_s = args.structures * world * args.steps / (total_ms * 1e-3)
     mean_trace_ms = float(np.mean(trace_ms))
     stats = np.sum([r['stats'] for r in bc.plan.collect()], axis=0)
+    # one instrumented launch (outside the timed region): our own box/sphere tests per query
+    bc.plan.launch.options = _lib.LAUNCH_COUNT_TESTS
+    bc.plan.enqueue()
+    cstats = np.sum([r['stats'] for r in bc.plan.collect()], axis=0)
+    bc.plan.launch.options = 0
+    own = {"box_tests_per_query": float(cstats[_lib.STAT_BOX]) / max(1, cstats[_lib.STAT_QUERIES]),
+           "sphere_tests_per_query": float(cstats[_lib.STAT_SPHERE]) / max(1, cstats[_lib.STAT_QUERIES]),
+           "queries_per_ray": float(cstats[_lib.STAT_QUERIES]) / rays_step}
 
     # -- end to end through the public API (pinned host in, host results out) -----
     e2e_ms = []
@@ -413,7 +421,7 @@ def main():
                 "batched_over_plain": (value / world / plain['rays_per_s']) if plain else None,
                 "ccs_rel_err_max_vs_fp64_oracle": ccs_err,
                 "grazing_queries": int(stats[_lib.STAT_GRAZING]), "fp64_fallback_queries": int(stats[_lib.STAT_FALLBACK]),
-                "queries": int(stats[_lib.STAT_QUERIES]),
+                "queries": int(stats[_lib.STAT_QUERIES]), "own_traversal": own,
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line), flush=True)

@@ -20,6 +20,7 @@ PREC_FP64, PREC_FP32 = 0, 1
 STAT_BOX, STAT_SPHERE, STAT_QUERIES, STAT_GRAZING, STAT_FALLBACK, STAT_FP64, STAT_ERRORS = range(7)
 NSTATS = 8
 BLOCK_EHSS, BLOCK_PA = 1, 2
+LAUNCH_COUNT_TESTS = 1
 FX_SCALE = 2.0 ** -40
 
 P = ct.c_void_p
@@ -33,7 +34,7 @@ class SceneInfo(ct.Structure):
 
 
 class Block(ct.Structure):
-    _fields_ = [('sv', (ct.c_uint32 * 4) * 30), ('shift', ct.c_uint32 * 4), ('scene', P), ('log2_rays', I32),
+    _fields_ = [('basis', (ct.c_uint32 * 4) * 30), ('base', ct.c_uint32 * 4), ('scene', P), ('log2_rays', I32),
                 ('cap', I32), ('precision', I32), ('flags', ct.c_uint32), ('hist_offset', I64),
                 ('chunk_begin', I64), ('reserved', I64)]
 
@@ -44,7 +45,8 @@ class BlockResult(ct.Structure):
 
 
 class Launch(ct.Structure):
-    _fields_ = [('block_threads', I32), ('ctas_per_sm', I32), ('chunk_rays', I32), ('reserved', I32)]
+    _fields_ = [('block_threads', I32), ('ctas_per_sm', I32), ('chunk_rays', I32), ('resolve_batch', I32),
+                ('precisions', I32), ('options', I32)]
 
 
 _SIGNATURES = {

@@ -24,7 +24,7 @@ import numpy as np
 from . import _lib
 from .device import empty, ptr, stream_handle, torch
 
-DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=8, chunk_rays=256)
+DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=5, chunk_rays=256, resolve_batch=8, count_tests=False)
 
 
 @dataclass
@@ -49,7 +49,12 @@ class BlockPlan:
         self.device = jobs[0].scene.device if device is None else device
         L = dict(DEFAULT_LAUNCH)
         L.update(launch or {})
-        self.launch = _lib.Launch(int(L['block_threads']), int(L['ctas_per_sm']), int(L['chunk_rays']), 0)
+        precisions = 0
+        for j in jobs:
+            precisions |= 1 << int(j.precision)
+        self.launch = _lib.Launch(int(L['block_threads']), int(L['ctas_per_sm']), int(L['chunk_rays']),
+                                  int(L['resolve_batch']), precisions,
+                                  _lib.LAUNCH_COUNT_TESTS if L['count_tests'] else 0)
         n = len(self.jobs)
         host = (_lib.Block * n)()
         seeds = (ct.c_uint64 * n)()

@@ -208,12 +208,13 @@ int ehss_blocks_prepare(ehss_block* blocks, int n_blocks, const uint64_t* seeds,
         if (!(B.flags & (EHSS_BLOCK_EHSS | EHSS_BLOCK_PA))) { set_error("block %d: no work flags", b); return EHSS_ERR_VALUE; }
         if (B.hist_offset < 0) B.hist_offset = hist;
         hist = B.hist_offset + B.cap + 1;
-        Sobol4Params p;
-        sobol4_params(seeds[b], &p);
-        for (int k = 0; k < 30; ++k) {
-            B.sv[k][0] = p.sv[k].x; B.sv[k][1] = p.sv[k].y; B.sv[k][2] = p.sv[k].z; B.sv[k][3] = p.sv[k].w;
+        uint32_t sv[4 * 30], shift[4];
+        sobol_scramble(4, seeds[b], sv, shift);
+        if (!sobol_coherent_order(B.log2_rays, sv, shift, &B.basis[0][0], B.base)) {
+            set_error("block %d: no coherent enumeration", b);
+            return EHSS_ERR_VALUE;
         }
-        B.shift[0] = p.shift.x; B.shift[1] = p.shift.y; B.shift[2] = p.shift.z; B.shift[3] = p.shift.w;
+        B.reserved = 0;
         B.chunk_begin = total;
         int64_t n = 1ll << B.log2_rays;
         total += (n + chunk_rays - 1) / chunk_rays;
@@ -239,8 +240,8 @@ int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_
     }
     if (workspace_bytes < 256) { set_error("blocks workspace must hold 256 bytes"); return EHSS_ERR_CAPACITY; }
     const ehss_launch& L = *launch;
-    if (L.block_threads < 64 || L.block_threads > 256 || L.block_threads % 32) {
-        set_error("block_threads must be a multiple of 32 in 64..256");
+    if (L.block_threads != 128) {
+        set_error("block_threads must be 128");
         return EHSS_ERR_VALUE;
     }
     if (L.ctas_per_sm < 1 || L.ctas_per_sm > 32) { set_error("ctas_per_sm must be 1..32"); return EHSS_ERR_VALUE; }
@@ -248,6 +249,8 @@ int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_
         set_error("chunk_rays must be a power of two in 32..4096");
         return EHSS_ERR_VALUE;
     }
+    if (L.resolve_batch < 1 || L.resolve_batch > 32) { set_error("resolve_batch must be 1..32"); return EHSS_ERR_VALUE; }
+    if (L.precisions < 0 || L.precisions > 3) { set_error("precisions must be a mask of 1 and 2 (0 = both)"); return EHSS_ERR_VALUE; }
     cudaStream_t s = as_stream(stream);
     int rc = cuda_status(cudaMemsetAsync(results_dev, 0, sizeof(ehss_block_result) * (size_t)n_blocks, s), "result reset");
     if (!rc && hist_entries > 0) rc = cuda_status(cudaMemsetAsync(hist_dev, 0, 8ull * hist_entries, s), "hist reset");

@@ -51,7 +51,7 @@ struct alignas(256) SceneHeader {
     uint64_t bytes;
 };
 static_assert(sizeof(SceneHeader) == 256, "scene header is one 256-byte line");
-static_assert(sizeof(ehss_block) % 16 == 0 && offsetof(ehss_block, sv) == 0 && offsetof(ehss_block, shift) == 480,
+static_assert(sizeof(ehss_block) % 16 == 0 && offsetof(ehss_block, basis) == 0 && offsetof(ehss_block, base) == 480,
               "block descriptors are read with 16-byte vector loads");
 
 struct SceneView {
@@ -215,6 +215,7 @@ __device__ __forceinline__ Ray64 impact_ray(uint4 q, const double* center, doubl
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
 bool sobol_scramble(int dim, uint64_t seed, uint32_t* sv, uint32_t* shift);
+bool sobol_coherent_order(int m, const uint32_t* sv, const uint32_t* shift, uint32_t* basis, uint32_t* base);
 void sobol_direction_numbers(int dim, uint32_t* v);
 int sm_count();
 void sobol4_params(uint64_t seed, Sobol4Params* p);

@@ -165,3 +165,90 @@ bool sobol_scramble(int dim, uint64_t seed, uint32_t* sv, uint32_t* shift) {
 }
 
 }  // namespace ehss
+
+namespace ehss {
+
+// Coherent enumeration of one block's 2^m Sobol(4) points.
+//
+// Point n is q(n) = shift ^ XOR_k n_k D[k] with D[k] = sv[k] ^ sv[k-1] (the
+// Gray-code recurrence written on the bits of n).  Rows "bit b of dimension
+// j" of this linear map are taken greedily, coarsest digits first and the
+// four dimensions in turn, keeping each row that is independent of those
+// already taken, until m rows form an invertible matrix A (always possible:
+// the leading m digits of dimension 0 alone are a bijection).  Position p is
+// given the point whose selected digits equal the bits of p (first row = most
+// significant bit of p): n = A^-1 (p ^ s), so consecutive positions differ
+// only in the finest selected digits and a warp's rays have nearby directions
+// and impact points.  The positions 0..2^m-1 enumerate exactly the same point
+// set as the indices 0..2^m-1.  Output: point(p) = base ^ XOR_{bit e of p}
+// basis[e] (dimension-major: basis[e*4 + j]).
+bool sobol_coherent_order(int m, const uint32_t* sv /* [4*30] dim-major */, const uint32_t* shift /* [4] */,
+                          uint32_t* basis /* [30*4] */, uint32_t* base /* [4] */) {
+    if (m < 0 || m > 30) return false;
+    constexpr int kDims = 4;
+    uint32_t D[kDims][kBits];
+    for (int j = 0; j < kDims; ++j)
+        for (int k = 0; k < kBits; ++k) D[j][k] = sv[j * kBits + k] ^ (k > 0 ? sv[j * kBits + k - 1] : 0u);
+    // candidate rows in preferred order; row = m-bit mask over n's bits
+    uint32_t rows[kBits];        // selected rows as bit masks over n (bit k <-> n_k)
+    uint32_t rshift[kBits];      // shift bit of each selected row
+    uint32_t echelon[kBits];     // reduced copies for the independence test
+    int pivot[kBits];
+    int taken = 0;
+    for (int b = 0; b < kBits && taken < m; ++b)
+        for (int j = 0; j < kDims && taken < m; ++j) {
+            uint32_t row = 0;
+            for (int k = 0; k < m; ++k) row |= ((D[j][k] >> (kBits - 1 - b)) & 1u) << k;
+            uint32_t red = row;
+            for (int t = 0; t < taken; ++t)
+                if ((red >> pivot[t]) & 1u) red ^= echelon[t];
+            if (!red) continue;
+            int pv = 31 - __builtin_clz(red);
+            echelon[taken] = red;
+            pivot[taken] = pv;
+            rows[taken] = row;
+            rshift[taken] = (shift[j] >> (kBits - 1 - b)) & 1u;
+            ++taken;
+        }
+    if (taken < m) return false;
+    // invert A (rows[t] . n = y_t) by Gauss-Jordan on [A | I]
+    uint32_t a[kBits], inv[kBits];
+    for (int t = 0; t < m; ++t) { a[t] = rows[t]; inv[t] = 1u << t; }
+    for (int col = 0; col < m; ++col) {
+        int r = col;
+        while (r < m && !((a[r] >> col) & 1u)) ++r;
+        if (r == m) return false;
+        uint32_t ta = a[r], ti = inv[r];
+        a[r] = a[col]; inv[r] = inv[col]; a[col] = ta; inv[col] = ti;
+        for (int q = 0; q < m; ++q)
+            if (q != col && ((a[q] >> col) & 1u)) { a[q] ^= a[col]; inv[q] ^= inv[col]; }
+    }
+    // now n_k = XOR_t inv[k]_t y_t ; y_t = bit (m-1-t) of p ^ rshift[t]
+    auto apply = [&](uint32_t nbits, uint32_t* out) {      // out[j] = XOR_k n_k D[j][k]
+        for (int j = 0; j < kDims; ++j) {
+            uint32_t v = 0;
+            for (int k = 0; k < m; ++k)
+                if ((nbits >> k) & 1u) v ^= D[j][k];
+            out[j] = v;
+        }
+    };
+    auto n_of_y = [&](uint32_t ybits) {                    // ybits bit t = y_t
+        uint32_t n = 0;
+        for (int k = 0; k < m; ++k)
+            n |= (uint32_t)(__builtin_popcount(inv[k] & ybits) & 1) << k;
+        return n;
+    };
+    uint32_t s = 0;
+    for (int t = 0; t < m; ++t) s |= rshift[t] << t;
+    uint32_t c[kDims];
+    apply(n_of_y(s), c);
+    for (int j = 0; j < kDims; ++j) base[j] = shift[j] ^ c[j];
+    for (int e = 0; e < kBits; ++e) {
+        uint32_t col[kDims] = {0, 0, 0, 0};
+        if (e < m) apply(n_of_y(1u << (m - 1 - e)), col);
+        for (int j = 0; j < kDims; ++j) basis[e * kDims + j] = col[j];
+    }
+    return true;
+}
+
+}  // namespace ehss

@@ -89,7 +89,7 @@ __device__ __forceinline__ bool better(double dist, int id, double best, int bes
 }
 
 // FP64 all-atom nearest search (origins far from the structure).
-__device__ int nearest_flat(const SceneView& S, const double* o, const double* d, int last_rank, double& best_out,
+__device__ __noinline__ int nearest_flat(const SceneView& S, const double* o, const double* d, int last_rank, double& best_out,
                             LocalStats& st) {
     int n = S.h->n_atoms;
     double best = CUDART_INF;
@@ -109,8 +109,8 @@ __device__ int nearest_flat(const SceneView& S, const double* o, const double* d
 // Nearest entry: returns the leaf-order rank of the collider (or -1) and its
 // FP64 entry distance, identical to the reference's choice.
 template <bool EXACT>
-__device__ int nearest(const SceneView& S, const double* o, const double* d, int last_rank, double& best_out,
-                       LocalStats& st) {
+__device__ __noinline__ int nearest(const SceneView& S, const double* o, const double* d, int last_rank,
+                                    double& best_out, LocalStats& st) {
     ++st.queries;
     RayF r;
     if (!setup_ray(S.h, o, d, r)) return nearest_flat(S, o, d, last_rank, best_out, st);
@@ -237,7 +237,8 @@ __device__ int nearest(const SceneView& S, const double* o, const double* d, int
 
 // Any-hit PA query (pa_spatial._one with sphere_hit): true when the ray
 // meets any sphere other than owner_rank.
-__device__ bool anyhit(const SceneView& S, const double* o, const double* d, int owner_rank, LocalStats& st) {
+__device__ __noinline__ bool anyhit(const SceneView& S, const double* o, const double* d, int owner_rank,
+                                    LocalStats& st) {
     ++st.queries;
     RayF r;
     if (!setup_ray(S.h, o, d, r)) {
@@ -427,10 +428,32 @@ __global__ void k_source_rays(const void* scene, Sobol4Params p, int64_t first, 
 
 // --------------------------------------------------------------------------
 // Fused blocks (persistent): Sobol -> impact disk -> EHSS / PA -> reduction
+//
+// One warp takes one chunk (chunk_rays consecutive positions of one block's
+// coherent Sobol enumeration) at a time.  Lanes are refilled with the chunk's
+// next ray as soon as theirs finishes.  Each warp alternates two phases:
+//   traverse  while-while walk (inner nodes, then postponed leaves) for every
+//             lane whose query is open, until at least `resolve_batch` lanes
+//             have finished their query or none is left traversing;
+//   resolve   for all finished lanes together: FP64 candidate re-test,
+//             escape / cap / reflection, and new rays for finished rays.
+// Batching the FP64 work keeps most lanes of the warp busy in both phases.
+// The FP64 ray state (position, direction, incoming direction) waits in
+// shared memory while the lane traverses in FP32.
 // --------------------------------------------------------------------------
-struct WarpBins {
+// Per-warp accumulators of the chunk in shared memory (updated once per ray
+// or per query, so registers stay free for the traversal).
+struct WarpAcc {
     unsigned count[kSmemBins];
     unsigned long long ledger[kSmemBins];
+    unsigned long long angle_fx;
+    unsigned hits, unresolved, escaped, pa;
+    unsigned queries, grazing, fallback, fp64, errors, pad;
+    unsigned long long box, sphere;
+};
+
+struct LaneRay {
+    double o[3], d[3], din[3];
 };
 
 __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long x) {
@@ -438,88 +461,320 @@ __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long x) {
     return x;
 }
 
-__global__ void __launch_bounds__(256) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
-                                                int chunk_rays, ehss_block_result* results, uint64_t* hist,
-                                                uint64_t* ledger, unsigned long long* work) {
-    extern __shared__ WarpBins bins_all[];
-    const unsigned lane = threadIdx.x & 31;
-    WarpBins& bins = bins_all[threadIdx.x >> 5];
+// Point at position p of a block's coherent enumeration.
+__device__ __forceinline__ uint4 block_point(const uint4* basis, uint4 base, uint32_t p) {
+    uint4 q = base;
+    while (p) {
+        int e = __ffs(p) - 1;
+        p &= p - 1;
+        uint4 v = __ldg(basis + e);
+        q.x ^= v.x; q.y ^= v.y; q.z ^= v.z; q.w ^= v.w;
+    }
+    return q;
+}
+
+constexpr int kIdle = 0, kTraverse = 1, kDone = 2, kNeedRay = 3;
+constexpr int kSentinel = INT32_MAX - 1;   // stack exhausted
+constexpr int kNoLeaf = INT32_MAX;
+
+template <bool EXACT, bool COUNT>
+struct Walker {
+    RayF r;
+    float U;
+    int cur, leaf, sp, steps;
+    int cand_rank[kCand];
+    float cand_lo[kCand];
+    bool overflow, grazing, error;
+    double best;
+    int best_rank, best_id;
+    unsigned box, sphere;
+    int stack_ref[kStackDepth];
+    float stack_t[kStackDepth];
+
+    __device__ __forceinline__ void reset() {
+        U = CUDART_INF_F;
+        cur = 0; leaf = kNoLeaf; sp = 0; steps = 0;
+#pragma unroll
+        for (int e = 0; e < kCand; ++e) { cand_rank[e] = -1; cand_lo[e] = CUDART_INF_F; }
+        overflow = grazing = error = false;
+        if (EXACT) { best = CUDART_INF; best_rank = -1; best_id = -1; }
+    }
+    __device__ __forceinline__ int pop() {
+        while (sp > 0) {
+            --sp;
+            if (stack_t[sp] <= U) return stack_ref[sp];
+        }
+        return kSentinel;
+    }
+    __device__ __forceinline__ int visit(const float4* nodes, int node) {
+        const float4* nd = nodes + 4 * (int64_t)node;
+        float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
+        if (COUNT) box += 2;
+        float t0 = box_enter(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, U);
+        float t1 = box_enter(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, U);
+        int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+        bool h0 = t0 != CUDART_INF_F && c0 != kEmpty, h1 = t1 != CUDART_INF_F && c1 != kEmpty;
+        if (h0 && h1) {
+            bool swap = t1 < t0;
+            if (sp < kStackDepth) { stack_ref[sp] = swap ? c0 : c1; stack_t[sp] = swap ? t0 : t1; ++sp; }
+            else error = true;
+            return swap ? c1 : c0;
+        }
+        if (h0) return c0;
+        if (h1) return c1;
+        return pop();
+    }
+    __device__ __forceinline__ void add_candidate(int k, float lo) {
+        if (lo > U) return;
+        bool placed = false;
+#pragma unroll
+        for (int e = 0; e < kCand; ++e) {
+            bool free_slot = cand_rank[e] < 0 || cand_lo[e] > U;
+            if (!placed && free_slot) { cand_rank[e] = k; cand_lo[e] = lo; placed = true; }
+        }
+        if (!placed) overflow = true;
+    }
+    __device__ __forceinline__ void leaf_tests(const SceneView& S, int ref, int last_rank, const LaneRay& L) {
+        int code = ~ref;
+        int first = code >> 3, cnt = (code & 7) + 1;
+        if (first + cnt > S.h->n_atoms) { error = true; return; }
+        for (int k = first; k < first + cnt; ++k) {
+            if (k == last_rank) continue;
+            if (COUNT) ++sphere;
+            if (EXACT) {
+                double4 a = S.atoms64[k];
+                double t = entry64(L.o[0], L.o[1], L.o[2], L.d[0], L.d[1], L.d[2], a.x, a.y, a.z, a.w);
+                int id = __ldg(S.ids + k);
+                if (better(t, id, best, best_id)) {
+                    best = t; best_rank = k; best_id = id;
+                    U = __double2float_ru(best);
+                }
+            } else {
+                float4 a = __ldg(S.atoms + k);
+                float vx = a.x - r.ox, vy = a.y - r.oy, vz = a.z - r.oz;
+                float b = fmaf(vx, r.dx, fmaf(vy, r.dy, vz * r.dz));
+                float px = fmaf(-b, r.dx, vx), py = fmaf(-b, r.dy, vy), pz = fmaf(-b, r.dz, vz);
+                float q = fmaf(px, px, fmaf(py, py, pz * pz));
+                float disc = fmaf(a.w, a.w, -q);
+                if (disc < -r.Edisc || b < -r.Ep) continue;
+                float s = sqrtf(fmaxf(disc, 0.0f));
+                float t = b - s;
+                if (disc >= 2.0f * r.Edisc) {
+                    float Et = 2.0f * (r.Ep + __fdividef(r.Edisc, s)) + 4.0f * kU32 * (fabsf(b) + s);
+                    if (t < -2.0f * Et) continue;
+                    if (t > Et) {
+                        float up = t + Et;
+                        if (up < U) U = up;
+                        add_candidate(k, t - Et);
+                        continue;
+                    }
+                }
+                grazing = true;
+                add_candidate(k, fmaxf(0.0f, (b - r.Ep - sqrtf(fmaxf(disc, 0.0f) + r.Edisc)) * (1.0f - 8.0f * kU32)));
+            }
+        }
+    }
+};
+
+// FP64 resolution of a finished FILTER query: re-test the candidates with the
+// reference formula and the (distance, id) rule.
+template <bool COUNT>
+__device__ __forceinline__ int resolve_candidates(const SceneView& S, const Walker<false, COUNT>& W, const LaneRay& L,
+                                                  double& best, unsigned& fp64) {
+    best = CUDART_INF;
+    int k = -1, best_id = -1;
+#pragma unroll
+    for (int e = 0; e < kCand; ++e) {
+        if (W.cand_rank[e] >= 0 && W.cand_lo[e] <= W.U) {
+            int kk = W.cand_rank[e];
+            double4 a = S.atoms64[kk];
+            double t = entry64(L.o[0], L.o[1], L.o[2], L.d[0], L.d[1], L.d[2], a.x, a.y, a.z, a.w);
+            ++fp64;
+            int id = __ldg(S.ids + kk);
+            if (better(t, id, best, best_id)) { best = t; k = kk; best_id = id; }
+        }
+    }
+    return k;
+}
+
+template <bool EXACT, bool COUNT>
+__global__ void __launch_bounds__(128, 5) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
+                                                   int chunk_rays, int resolve_batch, ehss_block_result* results,
+                                                   uint64_t* hist, uint64_t* ledger, unsigned long long* work) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    WarpAcc& A = reinterpret_cast<WarpAcc*>(smem_raw)[warp];
+    LaneRay& L = reinterpret_cast<LaneRay*>(smem_raw + sizeof(WarpAcc) * nwarps)[threadIdx.x];
+    const unsigned lt_mask = (1u << lane) - 1u;
+    Walker<EXACT, COUNT> W;
     while (true) {
         long long c = 0;
         if (lane == 0) c = (long long)atomicAdd(work, 1ull);
         c = __shfl_sync(0xffffffffu, c, 0);
         if (c >= total_chunks) break;
-        // block owning chunk c: last b with chunk_begin <= c
-        int lo = 0, hi = nb - 1;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (blocks[mid].chunk_begin <= c) lo = mid; else hi = mid - 1;
+        int bi = 0, hi = nb - 1;
+        while (bi < hi) {
+            int mid = (bi + hi + 1) >> 1;
+            if (blocks[mid].chunk_begin <= c) bi = mid; else hi = mid - 1;
         }
-        const ehss_block* B = blocks + lo;
-        const int log2n = B->log2_rays, cap = B->cap;
+        const ehss_block* B = blocks + bi;
+        if ((B->precision == EHSS_PREC_FP64) != EXACT) continue;     // the other instantiation's chunk
+        const int cap = B->cap;
         const uint32_t flags = B->flags;
-        const bool exact = B->precision == EHSS_PREC_FP64;
-        const int64_t n_rays = 1ll << log2n;
         const int64_t ray0 = (c - B->chunk_begin) * (int64_t)chunk_rays;
-        const int64_t cnt = min((int64_t)chunk_rays, n_rays - ray0);
-        const uint4* sv = reinterpret_cast<const uint4*>(B->sv);
-        const uint4 shift = make_uint4(B->shift[0], B->shift[1], B->shift[2], B->shift[3]);
-        SceneView S = scene_view(B->scene);
+        const int cnt = (int)min((long long)chunk_rays, (long long)((1ll << B->log2_rays) - ray0));
+        const SceneView S = scene_view(B->scene);
         const bool ok = S.h->magic == kSceneMagic && S.h->status == 0;
-        const double center[3] = {S.h->center[0], S.h->center[1], S.h->center[2]};
-        const double radius = S.h->radius;
-        if (lane < kSmemBins) { bins.count[lane] = 0; bins.ledger[lane] = 0; }
+        const int n_nodes = S.h->n_nodes;
+        if (lane < kSmemBins) { A.count[lane] = 0; A.ledger[lane] = 0; }
+        if (lane == 0) {
+            A.angle_fx = 0; A.hits = A.unresolved = A.escaped = A.pa = 0;
+            A.queries = A.grazing = A.fallback = A.fp64 = 0;
+            A.errors = ok ? 0 : 1;
+            A.box = A.sphere = 0;
+        }
         __syncwarp();
-        LocalStats st;
-        unsigned long long acc_fx = 0;
-        unsigned n_hits = 0, n_unres = 0, n_esc = 0, n_pa = 0;
-        for (int64_t j = lane; j < cnt && ok; j += 32) {
-            uint32_t idx = (uint32_t)(ray0 + j);
-            Ray64 ray = impact_ray(sobol4(sv, shift, idx), center, radius);
-            if (flags & EHSS_BLOCK_PA) n_pa += anyhit(S, ray.o, ray.d, -1, st);
-            if (flags & EHSS_BLOCK_EHSS) {
-                double din[3] = {ray.d[0], ray.d[1], ray.d[2]};
-                TraceOut t = trace_ray(S, ray.o, ray.d, -1, 0, cap, exact, nullptr, st);
-                unsigned long long fx = 0;
-                if (t.escaped) {
-                    double a = scatter_angle(din[0], din[1], din[2], ray.d[0], ray.d[1], ray.d[2]);
-                    fx = __double2ull_rn(a * 0x1p40);
-                    ++n_esc;
-                }
-                acc_fx += fx;
-                n_hits += (t.bounces > 0) || t.unresolved;
-                n_unres += t.unresolved;
-                int64_t k = t.bounces;
-                if (k < kSmemBins) {
-                    atomicAdd(&bins.count[k], 1u);
-                    if (fx) atomicAdd(&bins.ledger[k], fx);
+        if (COUNT) { W.box = 0; W.sphere = 0; }
+        int status = ok ? kNeedRay : kIdle;
+        int pool = 0, bounces = 0, last_rank = -1;
+        while (true) {
+            // ---- resolve finished queries (FP64) ----
+            if (status == kDone) {
+                int k;
+                double best;
+                if (W.error) {
+                    atomicAdd(&A.errors, 1u);
+                    k = -1; best = CUDART_INF;
+                } else if (EXACT) {
+                    k = W.best_rank; best = W.best;
+                    atomicAdd(&A.fp64, 1u);
                 } else {
-                    atomicAdd((unsigned long long*)&hist[B->hist_offset + k], 1ull);
-                    if (fx) atomicAdd((unsigned long long*)&ledger[B->hist_offset + k], fx);
+                    if (W.grazing) atomicAdd(&A.grazing, 1u);
+                    if (W.overflow) {
+                        LocalStats fst;
+                        k = nearest<true>(S, L.o, L.d, last_rank, best, fst);
+                        atomicAdd(&A.fallback, 1u);
+                        atomicAdd(&A.fp64, fst.fp64);
+                    } else {
+                        unsigned f = 0;
+                        k = resolve_candidates<COUNT>(S, reinterpret_cast<const Walker<false, COUNT>&>(W), L, best, f);
+                        atomicAdd(&A.fp64, f);
+                    }
+                }
+                if (k < 0 || bounces >= cap) {
+                    bool escaped = k < 0;
+                    unsigned long long fx = 0;
+                    if (escaped) {
+                        double a = scatter_angle(L.din[0], L.din[1], L.din[2], L.d[0], L.d[1], L.d[2]);
+                        fx = __double2ull_rn(a * 0x1p40);
+                        atomicAdd(&A.escaped, 1u);
+                        if (fx) atomicAdd(&A.angle_fx, fx);
+                    } else {
+                        atomicAdd(&A.unresolved, 1u);
+                    }
+                    if (bounces > 0 || !escaped) atomicAdd(&A.hits, 1u);
+                    if (bounces < kSmemBins) {
+                        atomicAdd(&A.count[bounces], 1u);
+                        if (fx) atomicAdd(&A.ledger[bounces], fx);
+                    } else {
+                        atomicAdd((unsigned long long*)&hist[B->hist_offset + bounces], 1ull);
+                        if (fx) atomicAdd((unsigned long long*)&ledger[B->hist_offset + bounces], fx);
+                    }
+                    status = kNeedRay;
+                } else {
+                    double4 a = S.atoms64[k];
+                    reflect64(L.o[0], L.o[1], L.o[2], L.d[0], L.d[1], L.d[2], a.x, a.y, a.z, a.w, best);
+                    ++bounces;
+                    last_rank = k;
+                    W.reset();
+                    if (!setup_ray(S.h, L.o, L.d, W.r)) W.error = true;   // bounce points lie within S
+                    atomicAdd(&A.queries, 1u);
+                    status = kTraverse;
                 }
             }
+            // ---- new rays for lanes whose ray finished ----
+            unsigned need = __ballot_sync(0xffffffffu, status == kNeedRay);
+            if (need) {
+                if (status == kNeedRay) {
+                    int p = pool + __popc(need & lt_mask);
+                    if (p < cnt) {
+                        const uint4 base = make_uint4(B->base[0], B->base[1], B->base[2], B->base[3]);
+                        uint4 q = block_point(reinterpret_cast<const uint4*>(B->basis), base, (uint32_t)(ray0 + p));
+                        Ray64 ray = impact_ray(q, S.h->center, S.h->radius);
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) { L.o[i] = ray.o[i]; L.d[i] = ray.d[i]; L.din[i] = ray.d[i]; }
+                        if (flags & EHSS_BLOCK_PA) {
+                            LocalStats pst;
+                            if (anyhit(S, L.o, L.d, -1, pst)) atomicAdd(&A.pa, 1u);
+                        }
+                        bounces = 0;
+                        last_rank = -1;
+                        if (flags & EHSS_BLOCK_EHSS) {
+                            W.reset();
+                            if (!setup_ray(S.h, L.o, L.d, W.r)) W.error = true;
+                            atomicAdd(&A.queries, 1u);
+                            status = kTraverse;
+                        }
+                    } else {
+                        status = kIdle;
+                    }
+                }
+                pool += __popc(need);
+                if (__any_sync(0xffffffffu, status == kNeedRay)) continue;   // PA-only lanes refill again
+            }
+            if (!__any_sync(0xffffffffu, status == kTraverse)) break;
+            // ---- traverse until enough queries are finished ----
+            while (true) {
+                if (status == kTraverse) {
+                    // inner nodes; the first leaf reached is postponed
+                    while (W.cur >= 0 && W.cur != kSentinel) {
+                        if (W.cur >= n_nodes || ++W.steps > 2 * n_nodes + 2) { W.error = true; W.cur = kSentinel; break; }
+                        W.cur = W.visit(S.nodes, W.cur);
+                        if (W.cur < 0 && W.leaf == kNoLeaf) {
+                            W.leaf = W.cur;
+                            W.cur = W.pop();
+                        }
+                        if (!__any_sync(__activemask(), W.leaf == kNoLeaf)) break;
+                    }
+                    // postponed leaf, then any leaf that comes next
+                    while (W.leaf != kNoLeaf) {
+                        W.leaf_tests(S, W.leaf, last_rank, L);
+                        W.leaf = kNoLeaf;
+                        if (W.cur < 0) {
+                            W.leaf = W.cur;
+                            W.cur = W.pop();
+                        }
+                    }
+                    if (W.cur == kSentinel) status = kDone;
+                }
+                unsigned done = __ballot_sync(0xffffffffu, status == kDone);
+                unsigned trav = __ballot_sync(0xffffffffu, status == kTraverse);
+                if (!trav || __popc(done) >= resolve_batch) break;
+            }
         }
-        if (!ok && lane == 0) ++st.errors;
-        // warp reduction of the chunk, then one atomic per field into the block result
-        unsigned long long s_fx = warp_sum64(acc_fx);
-        unsigned s_hits = __reduce_add_sync(0xffffffffu, n_hits);
-        unsigned s_unres = __reduce_add_sync(0xffffffffu, n_unres);
-        unsigned s_esc = __reduce_add_sync(0xffffffffu, n_esc);
-        unsigned s_pa = __reduce_add_sync(0xffffffffu, n_pa);
-        ehss_block_result* R = results + lo;
-        if (lane == 0) {
-            if (s_fx) atomicAdd((unsigned long long*)&R->angle_fx, s_fx);
-            if (s_hits) atomicAdd((unsigned long long*)&R->hits, (unsigned long long)s_hits);
-            if (s_unres) atomicAdd((unsigned long long*)&R->unresolved, (unsigned long long)s_unres);
-            if (s_esc) atomicAdd((unsigned long long*)&R->escaped, (unsigned long long)s_esc);
-            if (s_pa) atomicAdd((unsigned long long*)&R->pa_blocked, (unsigned long long)s_pa);
+        if (COUNT) {
+            unsigned long long b = warp_sum64(W.box), sp = warp_sum64(W.sphere);
+            if (lane == 0) { A.box = b; A.sphere = sp; }
         }
-        flush_stats(st, R->stats);
         __syncwarp();
+        // one atomic per field into the block result
+        ehss_block_result* R = results + bi;
+        if (lane == 0) {
+            if (A.angle_fx) atomicAdd((unsigned long long*)&R->angle_fx, A.angle_fx);
+            if (A.hits) atomicAdd((unsigned long long*)&R->hits, (unsigned long long)A.hits);
+            if (A.unresolved) atomicAdd((unsigned long long*)&R->unresolved, (unsigned long long)A.unresolved);
+            if (A.escaped) atomicAdd((unsigned long long*)&R->escaped, (unsigned long long)A.escaped);
+            if (A.pa) atomicAdd((unsigned long long*)&R->pa_blocked, (unsigned long long)A.pa);
+            unsigned long long v[7] = {A.box, A.sphere, A.queries, A.grazing, A.fallback, A.fp64, A.errors};
+            const int slot[7] = {EHSS_STAT_BOX_TESTS, EHSS_STAT_SPHERE_TESTS, EHSS_STAT_QUERIES, EHSS_STAT_GRAZING,
+                                 EHSS_STAT_FALLBACK, EHSS_STAT_FP64_TESTS, EHSS_STAT_ERRORS};
+            for (int i = 0; i < 7; ++i)
+                if (v[i]) atomicAdd((unsigned long long*)&R->stats[slot[i]], v[i]);
+        }
         if (lane < kSmemBins && lane <= cap) {
-            if (bins.count[lane])
-                atomicAdd((unsigned long long*)&hist[B->hist_offset + lane], (unsigned long long)bins.count[lane]);
-            if (bins.ledger[lane]) atomicAdd((unsigned long long*)&ledger[B->hist_offset + lane], bins.ledger[lane]);
+            if (A.count[lane])
+                atomicAdd((unsigned long long*)&hist[B->hist_offset + lane], (unsigned long long)A.count[lane]);
+            if (A.ledger[lane]) atomicAdd((unsigned long long*)&ledger[B->hist_offset + lane], A.ledger[lane]);
         }
         __syncwarp();
     }
@@ -568,11 +823,30 @@ int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const 
                   ehss_block_result* results, uint64_t* hist, uint64_t* ledger, unsigned long long* work,
                   cudaStream_t stream) {
     int warps = L.block_threads / 32;
-    size_t smem = sizeof(WarpBins) * (size_t)warps;
+    size_t smem = sizeof(WarpAcc) * (size_t)warps + sizeof(LaneRay) * (size_t)L.block_threads;
     unsigned grid = (unsigned)(sm_count() * L.ctas_per_sm);
-    k_blocks<<<grid, L.block_threads, smem, stream>>>(blocks, nb, total_chunks, L.chunk_rays, results, hist, ledger,
-                                                      work);
-    return cuda_status(cudaGetLastError(), "blocks launch");
+    int batch = L.resolve_batch > 0 ? L.resolve_batch : 1;
+    const bool count = (L.options & EHSS_LAUNCH_COUNT_TESTS) != 0;
+    // one launch per precision present; each skips the other precision's chunks
+    const int mask = L.precisions ? L.precisions : 3;
+    bool first = true;
+    for (int exact = 1; exact >= 0; --exact) {
+        if (!((mask >> (exact ? EHSS_PREC_FP64 : EHSS_PREC_FP32)) & 1)) continue;
+        if (!first) {
+            int rc = cuda_status(cudaMemsetAsync(work, 0, 8, stream), "work counter reset");
+            if (rc) return rc;
+        }
+        first = false;
+#define EHSS_LAUNCH_BLOCKS(E, C) \
+        k_blocks<E, C><<<grid, L.block_threads, smem, stream>>>(blocks, nb, total_chunks, L.chunk_rays, batch, \
+                                                                results, hist, ledger, work)
+        if (exact) { if (count) EHSS_LAUNCH_BLOCKS(true, true); else EHSS_LAUNCH_BLOCKS(true, false); }
+        else { if (count) EHSS_LAUNCH_BLOCKS(false, true); else EHSS_LAUNCH_BLOCKS(false, false); }
+#undef EHSS_LAUNCH_BLOCKS
+        int rc = cuda_status(cudaGetLastError(), "blocks launch");
+        if (rc) return rc;
+    }
+    return EHSS_OK;
 }
 
 }  // namespace ehss

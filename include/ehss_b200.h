@@ -172,11 +172,18 @@ int ehss_pa_anyhit(const void* scene_dev, int64_t n_rays, const double* origins_
 #define EHSS_BLOCK_EHSS 1u      /* trace EHSS */
 #define EHSS_BLOCK_PA 2u        /* any-hit PA on the same rays */
 
-/* 544 bytes, a multiple of 16: the device reads sv/shift as 16-byte vectors,
- * so a device array of blocks must start on a 16-byte boundary. */
+/* 544 bytes, a multiple of 16: the device reads basis/base as 16-byte
+ * vectors, so a device array of blocks must start on a 16-byte boundary.
+ * ehss_blocks_prepare fills basis/base with the block's 2^log2_rays Sobol(4)
+ * points of `seed` in a spatially coherent enumeration: position p carries
+ * the point (base ^ XOR_{bit e of p} basis[e]) * 2^-30.  The positions
+ * 0..2^log2_rays-1 enumerate exactly the scipy point set of (seed,
+ * log2_rays), reordered so that neighbouring positions share their leading
+ * digits (nearby directions and impact points); block sums do not depend on
+ * the order. */
 typedef struct ehss_block {
-    uint32_t sv[30][4];       /* Sobol(4) direction numbers, [bit][dim] (offset 0) */
-    uint32_t shift[4];        /* offset 480 */
+    uint32_t basis[30][4];    /* per position bit, [bit][dim] (offset 0) */
+    uint32_t base[4];         /* offset 480 */
     const void* scene;        /* device scene buffer */
     int32_t log2_rays;        /* 3..24 */
     int32_t cap;              /* collision cap >= 1 */
@@ -208,10 +215,14 @@ int ehss_blocks_workspace_bytes(int n_blocks, uint64_t* bytes);
 typedef struct ehss_launch {
     int32_t block_threads;    /* 64..256, multiple of 32 */
     int32_t ctas_per_sm;      /* persistent CTAs per SM (grid = SMs * ctas_per_sm) */
-    int32_t chunk_rays;       /* rays per work item (as passed to ehss_blocks_prepare); each
-                                 lane of the warp that takes the item traces chunk_rays/32 rays */
-    int32_t reserved;         /* 0 */
+    int32_t chunk_rays;       /* rays per work item (as passed to ehss_blocks_prepare) */
+    int32_t resolve_batch;    /* a warp leaves its traversal phase once this many lanes have a
+                                 finished query, and resolves them together (1..32) */
+    int32_t precisions;       /* bit mask of the EHSS_PREC_* values present among the blocks
+                                 (1 << EHSS_PREC_FP64 | 1 << EHSS_PREC_FP32); 0 = both */
+    int32_t options;          /* EHSS_LAUNCH_* bits */
 } ehss_launch;
+#define EHSS_LAUNCH_COUNT_TESTS 1   /* count box and sphere tests into the block stats (slower) */
 
 /* Run all blocks in one persistent launch.  blocks_dev: device copy of the
  * prepared descriptors; results_dev[n_blocks], hist_dev/ledger_dev

@@ -77,9 +77,6 @@ def test_blocks_prepare_chunks_and_offsets(lib):
     assert total.value == 16 + 1 + 64
     assert [b.chunk_begin for b in blocks] == [0, 16, 17]
     assert [b.hist_offset for b in blocks] == [0, 65, 67]
-    sv, sh = O.sobol_scramble(4, 2)
-    np.testing.assert_array_equal(np.array([[blocks[2].sv[k][j] for j in range(4)] for k in range(30)]), sv.T)
-    np.testing.assert_array_equal(np.array(blocks[2].shift[:]), sh)
     blocks[1].cap = 0
     assert lib.ehss_blocks_prepare(blocks, n, seeds, 256, ct.byref(total)) == _lib.ERR_VALUE
     assert lib.ehss_blocks_prepare(blocks, n, seeds, 100, ct.byref(total)) == _lib.ERR_VALUE
@@ -87,9 +84,9 @@ def test_blocks_prepare_chunks_and_offsets(lib):
 
 def test_struct_layouts_match_header():
     from ehss_b200 import _lib
-    assert ct.sizeof(_lib.Block) == 544 and _lib.Block.sv.offset == 0 and _lib.Block.shift.offset == 480
+    assert ct.sizeof(_lib.Block) == 544 and _lib.Block.basis.offset == 0 and _lib.Block.base.offset == 480
     assert ct.sizeof(_lib.BlockResult) == 8 * (5 + _lib.NSTATS)
-    assert ct.sizeof(_lib.Launch) == 16
+    assert ct.sizeof(_lib.Launch) == 24
 
 
 def test_workload_generators():
@@ -126,3 +123,33 @@ def test_state_types_validate_like_reference():
         EHSSSource(np.zeros((1, 3)), 2 * d, d, np.ones(1), np.array([-1]), np.array([0]), 'x')
     with pytest.raises(ValueError):
         EHSSSource(np.zeros((1, 3)), d, d, np.ones(1), np.array([-1]), np.array([1]), 'x')
+
+
+@pytest.mark.parametrize('m,seed', [(3, 0), (8, 190003), (12, 7), (14, 2 ** 32 - 1), (16, 104729)])
+def test_coherent_enumeration_is_the_sobol_point_set(lib, m, seed):
+    """Block descriptors enumerate exactly scipy's points, neighbours close."""
+    from ehss_b200 import _lib
+    blocks = (_lib.Block * 1)()
+    blocks[0].scene = 0x1000
+    blocks[0].log2_rays = m
+    blocks[0].cap = 8
+    blocks[0].precision = 1
+    blocks[0].flags = _lib.BLOCK_EHSS
+    blocks[0].hist_offset = -1
+    total = ct.c_int64()
+    assert lib.ehss_blocks_prepare(blocks, 1, (ct.c_uint64 * 1)(seed), 64, ct.byref(total)) == 0
+    basis = np.array([[blocks[0].basis[e][j] for j in range(4)] for e in range(30)], dtype=np.uint32)
+    base = np.array(blocks[0].base[:], dtype=np.uint32)
+    p = np.arange(1 << m, dtype=np.uint64)
+    pts = np.tile(base, (1 << m, 1))
+    for e in range(m):
+        sel = ((p >> np.uint64(e)) & np.uint64(1)).astype(bool)
+        pts[sel] ^= basis[e]
+    ref = O.sobol_integers(4, m, seed)
+    got_sorted = np.lexsort(pts.T[::-1]); ref_sorted = np.lexsort(ref.T[::-1])
+    np.testing.assert_array_equal(pts[got_sorted], ref[ref_sorted])
+    if m >= 12:
+        # the 32 positions of a warp share the leading digits of all four dimensions
+        digits = (m - 5) // 4
+        top = pts.reshape(-1, 32, 4) >> np.uint32(30 - digits)
+        assert (top == top[:, :1, :]).all(axis=(1, 2)).mean() == 1.0
