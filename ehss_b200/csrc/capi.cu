@@ -226,7 +226,7 @@ int ehss_blocks_prepare(ehss_block* blocks, int n_blocks, const uint64_t* seeds,
 int ehss_blocks_workspace_bytes(int n_blocks, uint64_t* bytes) {
     clear_error();
     if (n_blocks < 1 || !bytes) { set_error("invalid arguments"); return EHSS_ERR_VALUE; }
-    *bytes = 256;
+    *bytes = sizeof(unsigned long long) * kMaxWorkParts;
     return EHSS_OK;
 }
 
@@ -238,7 +238,10 @@ int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_
         set_error("invalid arguments");
         return EHSS_ERR_VALUE;
     }
-    if (workspace_bytes < 256) { set_error("blocks workspace must hold 256 bytes"); return EHSS_ERR_CAPACITY; }
+    if (workspace_bytes < sizeof(unsigned long long) * kMaxWorkParts) {
+        set_error("blocks workspace must hold %zu bytes", sizeof(unsigned long long) * kMaxWorkParts);
+        return EHSS_ERR_CAPACITY;
+    }
     const ehss_launch& L = *launch;
     if (L.block_threads != 128) {
         set_error("block_threads must be 128");
@@ -255,7 +258,8 @@ int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_
     int rc = cuda_status(cudaMemsetAsync(results_dev, 0, sizeof(ehss_block_result) * (size_t)n_blocks, s), "result reset");
     if (!rc && hist_entries > 0) rc = cuda_status(cudaMemsetAsync(hist_dev, 0, 8ull * hist_entries, s), "hist reset");
     if (!rc && hist_entries > 0) rc = cuda_status(cudaMemsetAsync(ledger_dev, 0, 8ull * hist_entries, s), "ledger reset");
-    if (!rc) rc = cuda_status(cudaMemsetAsync(workspace_dev, 0, 8, s), "work counter reset");
+    if (!rc) rc = cuda_status(cudaMemsetAsync(workspace_dev, 0, sizeof(unsigned long long) * kMaxWorkParts, s),
+                              "work counter reset");
     if (rc) return rc;
     if (total_chunks == 0) return EHSS_OK;
     return launch_blocks(blocks_dev, n_blocks, total_chunks, L, results_dev, hist_dev, ledger_dev,

@@ -13,24 +13,28 @@ namespace ehss {
 // Scene buffer layout (one structure, device resident, 256-byte aligned).
 //
 //   SceneHeader                              256 B
-//   nodes   float4[4 * n_nodes]              binary LBVH, both child boxes per node
+//   nodes   float4[8 * n_nodes]              4-wide nodes (below), child boxes in FP32
 //   atoms   float4[n]      (x, y, z, r)      FP32, centre relative to header.center,
 //                                            in leaf order
 //   atoms64 double4[n]     (x, y, z, r)      FP64 reference values, leaf order
 //   ids     int32[n]       leaf order -> input atom id
 //   rank    int32[n]       input atom id -> leaf order
 //
-// Node record (64 B, four float4):
-//   n0 = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
-//   n1 = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
-//   n2 = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
-//   n3 = (child0, child1, -, -) as int bits
-// child >= 0: internal node index; child < 0: leaf ~(first << 3 | (count - 1)).
-// An empty child carries an inverted box and is never entered.
+// Node record (128 B, eight float4): a 4-wide node, structure of arrays over
+// its children c = 0..3:
+//   f[0] = lo.x[c]  f[1] = hi.x[c]  f[2] = lo.y[c]  f[3] = hi.y[c]
+//   f[4] = lo.z[c]  f[5] = hi.z[c]  f[6] = child ref[c] (int bits)  f[7] = unused
+// child >= 0: node index; child < 0: leaf ~(first << 3 | (count - 1));
+// kEmptyChild marks an unused slot.  Node i is built from binary LBVH node i
+// with its grandchildren as children (children that are leaves, or subtrees
+// of at most leaf_size atoms, stay single slots), so only binary nodes at
+// even depth are ever referenced.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kSceneMagic = 0x45485353u;  // "EHSS"
 constexpr int kMaxLeaf = 8;
-constexpr int kStackDepth = 64;
+constexpr int kEmptyChild = INT32_MIN;
+constexpr int kStackDepth = 96;   // >= 3 x the deepest 4-wide tree (binary LBVH height <= 55)
+constexpr int kMaxWorkParts = 512;    // per-SM work ranges of the persistent kernel (workspace 4 KiB)
 
 struct alignas(256) SceneHeader {
     uint32_t magic;
@@ -69,7 +73,7 @@ inline void scene_layout(int64_t n, uint64_t* off_nodes, uint64_t* off_atoms, ui
                          uint64_t* off_ids, uint64_t* off_rank, uint64_t* total) {
     int64_t nodes = n > 1 ? n - 1 : 1;
     uint64_t o = 256;
-    *off_nodes = o; o = align256(o + (uint64_t)nodes * 64);
+    *off_nodes = o; o = align256(o + (uint64_t)nodes * 128);
     *off_atoms = o; o = align256(o + (uint64_t)n * 16);
     *off_atoms64 = o; o = align256(o + (uint64_t)n * 32);
     *off_ids = o; o = align256(o + (uint64_t)n * 4);

@@ -275,10 +275,23 @@ __global__ void k_refit(const BuildDesc* descs, const int32_t* atom_scene, int64
     }
 }
 
-__device__ __forceinline__ void put_child_box(float4& nxy, float& lz, float& hz, const float* b, float eps) {
-    nxy = make_float4(__fsub_rd(b[0], eps), __fadd_ru(b[3], eps), __fsub_rd(b[1], eps), __fadd_ru(b[4], eps));
-    lz = __fsub_rd(b[2], eps);
-    hz = __fadd_ru(b[5], eps);
+// 4-wide node record i (see ehss_internal.cuh) from up to four child slots.
+__device__ __forceinline__ void write_node4(float4* nodes, int64_t i, const float (*box)[6], const int* ref, int n,
+                                            float eps) {
+    float v[6][4];
+    int r[4];
+    for (int c = 0; c < 4; ++c) {
+        bool used = c < n;
+        for (int k = 0; k < 3; ++k) {
+            v[2 * k][c] = used ? __fsub_rd(box[c][k], eps) : 0.f;          // lo, rounded outward
+            v[2 * k + 1][c] = used ? __fadd_ru(box[c][3 + k], eps) : 0.f;  // hi
+        }
+        r[c] = used ? ref[c] : kEmptyChild;
+    }
+    float4* nd = nodes + 8 * i;
+    for (int f = 0; f < 6; ++f) nd[f] = make_float4(v[f][0], v[f][1], v[f][2], v[f][3]);
+    nd[6] = make_float4(__int_as_float(r[0]), __int_as_float(r[1]), __int_as_float(r[2]), __int_as_float(r[3]));
+    nd[7] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 __global__ void k_emit_nodes(const BuildDesc* descs, int n_scenes, int64_t I_total, const int32_t* inner_child,
@@ -297,19 +310,14 @@ __global__ void k_emit_nodes(const BuildDesc* descs, int n_scenes, int64_t I_tot
         }
         // whole structure in one leaf below a single node
         float4* nodes = reinterpret_cast<float4*>(D.scene + H->off_nodes);
-        float u[6] = {CUDART_INF_F, CUDART_INF_F, CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F};
+        float u[1][6] = {{CUDART_INF_F, CUDART_INF_F, CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F}};
         for (int64_t a = 0; a < D.n; ++a)
             for (int k = 0; k < 3; ++k) {
-                u[k] = fminf(u[k], leaf_box[6 * (D.atom0 + a) + k]);
-                u[3 + k] = fmaxf(u[3 + k], leaf_box[6 * (D.atom0 + a) + 3 + k]);
+                u[0][k] = fminf(u[0][k], leaf_box[6 * (D.atom0 + a) + k]);
+                u[0][3 + k] = fmaxf(u[0][3 + k], leaf_box[6 * (D.atom0 + a) + 3 + k]);
             }
-        float4 n0; float lz, hz;
-        put_child_box(n0, lz, hz, u, H->eps_box);
-        nodes[0] = n0;
-        nodes[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-        nodes[2] = make_float4(lz, hz, 0.f, 0.f);
-        int leaf = ~((0 << 3) | (int)(D.n - 1));
-        nodes[3] = make_float4(__int_as_float(leaf), __int_as_float(INT32_MIN), 0.f, 0.f);
+        int ref = ~((0 << 3) | (int)(D.n - 1));
+        write_node4(nodes, 0, u, &ref, 1, H->eps_box);
         H->depth = 1;
         H->n_nodes = 1;
         return;
@@ -323,29 +331,46 @@ __global__ void k_emit_nodes(const BuildDesc* descs, int n_scenes, int64_t I_tot
     int i = (int)(g - D.inner0);
     if (i >= D.n - 1 || D.n <= D.leaf_size) return;
     SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
-    float4* nodes = reinterpret_cast<float4*>(D.scene + H->off_nodes) + 4 * (int64_t)i;
-    float eps = H->eps_box;
-    int refs[2];
-    float4 nxy[2];
-    float lz[2], hz[2];
-    for (int side = 0; side < 2; ++side) {
-        int c = inner_child[2 * g + side];
-        const float* box;
+    float4* nodes = reinterpret_cast<float4*>(D.scene + H->off_nodes);
+    // slot of a binary child: leaf reference when it is an atom or a subtree
+    // of at most leaf_size atoms, else the node index (expanded once more)
+    auto classify = [&](int c, int& ref, const float*& box) -> bool {   // true: expandable internal node
         if (c < 0) {
             box = leaf_box + 6 * (D.atom0 + ~c);
-            refs[side] = ~((~c) << 3);                    // one atom
-        } else {
-            box = inner_box + 6 * (D.inner0 + c);
-            int first = inner_range[2 * (D.inner0 + c)], last = inner_range[2 * (D.inner0 + c) + 1];
-            int count = last - first + 1;
-            refs[side] = (count <= D.leaf_size) ? ~((first << 3) | (count - 1)) : c;
+            ref = ~((~c) << 3);
+            return false;
         }
-        put_child_box(nxy[side], lz[side], hz[side], box, eps);
+        box = inner_box + 6 * (D.inner0 + c);
+        int first = inner_range[2 * (D.inner0 + c)], last = inner_range[2 * (D.inner0 + c) + 1];
+        int count = last - first + 1;
+        if (count <= D.leaf_size) { ref = ~((first << 3) | (count - 1)); return false; }
+        ref = c;
+        return true;
+    };
+    int refs[4];
+    float boxes[4][6];
+    int n = 0;
+    for (int side = 0; side < 2; ++side) {
+        int c = inner_child[2 * g + side];
+        int ref;
+        const float* box;
+        if (!classify(c, ref, box)) {
+            refs[n] = ref;
+            for (int k = 0; k < 6; ++k) boxes[n][k] = box[k];
+            ++n;
+            continue;
+        }
+        for (int side2 = 0; side2 < 2; ++side2) {          // grandchildren
+            int gc = inner_child[2 * (D.inner0 + c) + side2];
+            int ref2;
+            const float* box2;
+            classify(gc, ref2, box2);
+            refs[n] = ref2;
+            for (int k = 0; k < 6; ++k) boxes[n][k] = box2[k];
+            ++n;
+        }
     }
-    nodes[0] = nxy[0];
-    nodes[1] = nxy[1];
-    nodes[2] = make_float4(lz[0], hz[0], lz[1], hz[1]);
-    nodes[3] = make_float4(__int_as_float(refs[0]), __int_as_float(refs[1]), 0.f, 0.f);
+    write_node4(nodes, i, boxes, refs, n, H->eps_box);
 }
 
 __global__ void k_emit_atoms(const BuildDesc* descs, const int32_t* atom_scene, int64_t N, const int32_t* vals_sorted) {

@@ -35,7 +35,6 @@ namespace ehss {
 
 constexpr float kU32 = 5.9604645e-08f;   // 2^-24
 constexpr int kCand = 4;
-constexpr int kEmpty = INT32_MIN;
 constexpr int kSmemBins = 16;
 
 struct LocalStats {
@@ -80,6 +79,40 @@ __device__ __forceinline__ float box_enter(const RayF& r, float lx, float hx, fl
     float tmin = fmaxf(fmaxf(fminf(tlx, thx), fminf(tly, thy)), fmaxf(fminf(tlz, thz), 0.0f));
     float tmax = fminf(fminf(fmaxf(tlx, thx), fmaxf(tly, thy)), fminf(fmaxf(tlz, thz), U));
     return tmin <= tmax ? tmin : CUDART_INF_F;
+}
+
+// One 4-wide node: entry distances of the children that the ray meets within
+// [0, U], sorted ascending (misses and empty slots last, at +inf).
+struct Hits4 {
+    int ref[4];
+    float t[4];
+    int n;
+};
+
+__device__ __forceinline__ void cswap(Hits4& h, int a, int b) {
+    bool s = h.t[b] < h.t[a];
+    float ta = s ? h.t[b] : h.t[a], tb = s ? h.t[a] : h.t[b];
+    int ra = s ? h.ref[b] : h.ref[a], rb = s ? h.ref[a] : h.ref[b];
+    h.t[a] = ta; h.t[b] = tb; h.ref[a] = ra; h.ref[b] = rb;
+}
+
+__device__ __forceinline__ Hits4 visit4(const float4* nodes, int node, const RayF& r, float U) {
+    const float4* nd = nodes + 8 * (int64_t)node;
+    float4 lx = __ldg(nd), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
+    float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5), rf = __ldg(nd + 6);
+    Hits4 h;
+    h.ref[0] = __float_as_int(rf.x); h.ref[1] = __float_as_int(rf.y);
+    h.ref[2] = __float_as_int(rf.z); h.ref[3] = __float_as_int(rf.w);
+    h.t[0] = box_enter(r, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, U);
+    h.t[1] = box_enter(r, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, U);
+    h.t[2] = box_enter(r, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, U);
+    h.t[3] = box_enter(r, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, U);
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        if (h.ref[c] == kEmptyChild) h.t[c] = CUDART_INF_F;
+    cswap(h, 0, 1); cswap(h, 2, 3); cswap(h, 0, 2); cswap(h, 1, 3); cswap(h, 1, 2);
+    h.n = (h.t[0] != CUDART_INF_F) + (h.t[1] != CUDART_INF_F) + (h.t[2] != CUDART_INF_F) + (h.t[3] != CUDART_INF_F);
+    return h;
 }
 
 // Reference rule of nearest_scalar (ehss_cpu.py:60): strictly nearer, or
@@ -132,25 +165,17 @@ __device__ __noinline__ int nearest(const SceneView& S, const double* o, const d
     for (int steps = 0;; ++steps) {
         if (cur >= n_nodes || steps > 2 * n_nodes + 2) { ++st.errors; break; }
         if (cur >= 0) {
-            const float4* nd = S.nodes + 4 * (int64_t)cur;
-            float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
-            st.box += 2;
-            float t0 = box_enter(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, U);
-            float t1 = box_enter(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, U);
-            int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
-            bool h0 = t0 != CUDART_INF_F, h1 = t1 != CUDART_INF_F;
-            if (h0 && h1) {
-                bool swap = t1 < t0;
-                int nearc = swap ? c1 : c0, farc = swap ? c0 : c1;
-                float fart = swap ? t0 : t1;
-                if (sp < kStackDepth) { stack_ref[sp] = farc; stack_t[sp] = fart; ++sp; }
-                else { ++st.errors; }
-                cur = nearc;
+            Hits4 h = visit4(S.nodes, cur, r, U);
+            st.box += 4;
+            if (h.n > 0) {
+                for (int k = h.n - 1; k >= 1; --k) {
+                    if (sp < kStackDepth) { stack_ref[sp] = h.ref[k]; stack_t[sp] = h.t[k]; ++sp; }
+                    else { ++st.errors; }
+                }
+                cur = h.ref[0];
                 continue;
             }
-            if (h0) { cur = c0; continue; }
-            if (h1) { cur = c1; continue; }
-        } else if (cur != kEmpty) {
+        } else {
             int code = ~cur;
             int first = code >> 3, cnt = (code & 7) + 1;
             if (first + cnt > n_atoms) { ++st.errors; cnt = 0; }
@@ -259,20 +284,16 @@ __device__ __noinline__ bool anyhit(const SceneView& S, const double* o, const d
     for (int steps = 0;; ++steps) {
         if (cur >= n_nodes || steps > 2 * n_nodes + 2) { ++st.errors; break; }
         if (cur >= 0) {
-            const float4* nd = S.nodes + 4 * (int64_t)cur;
-            float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
-            st.box += 2;
-            bool h0 = box_enter(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, U) != CUDART_INF_F;
-            bool h1 = box_enter(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, U) != CUDART_INF_F;
-            int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
-            if (h0 && h1) {
-                if (sp < kStackDepth) stack_ref[sp++] = c1; else ++st.errors;
-                cur = c0;
+            Hits4 h = visit4(S.nodes, cur, r, U);
+            st.box += 4;
+            if (h.n > 0) {
+                for (int k = h.n - 1; k >= 1; --k) {
+                    if (sp < kStackDepth) stack_ref[sp++] = h.ref[k]; else ++st.errors;
+                }
+                cur = h.ref[0];
                 continue;
             }
-            if (h0) { cur = c0; continue; }
-            if (h1) { cur = c1; continue; }
-        } else if (cur != kEmpty) {
+        } else {
             int code = ~cur;
             int first = code >> 3, cnt = (code & 7) + 1;
             if (first + cnt > n_atoms) { ++st.errors; cnt = 0; }
@@ -477,6 +498,12 @@ constexpr int kIdle = 0, kTraverse = 1, kDone = 2, kNeedRay = 3;
 constexpr int kSentinel = INT32_MAX - 1;   // stack exhausted
 constexpr int kNoLeaf = INT32_MAX;
 
+// Traversal stack: the top kSmemStack entries of each lane live in shared
+// memory (entry i of lane t at smem_stack[i * blockDim + t], conflict-free);
+// deeper entries, rare for an LBVH walked near-child first, go to a
+// per-lane local array.
+constexpr int kSmemStack = 16;
+
 template <bool EXACT, bool COUNT>
 struct Walker {
     RayF r;
@@ -488,8 +515,17 @@ struct Walker {
     double best;
     int best_rank, best_id;
     unsigned box, sphere;
-    int stack_ref[kStackDepth];
-    float stack_t[kStackDepth];
+    int2* sstack;          // this lane's shared-memory stack column
+    int stride;            // entries are stride apart (blockDim.x)
+    int deep_ref[kStackDepth - kSmemStack];
+    float deep_t[kStackDepth - kSmemStack];
+
+    __device__ __forceinline__ void push(int ref, float t) {
+        if (sp < kSmemStack) sstack[sp * stride] = make_int2(ref, __float_as_int(t));
+        else if (sp < kStackDepth) { deep_ref[sp - kSmemStack] = ref; deep_t[sp - kSmemStack] = t; }
+        else { error = true; return; }
+        ++sp;
+    }
 
     __device__ __forceinline__ void reset() {
         U = CUDART_INF_F;
@@ -502,27 +538,22 @@ struct Walker {
     __device__ __forceinline__ int pop() {
         while (sp > 0) {
             --sp;
-            if (stack_t[sp] <= U) return stack_ref[sp];
+            int ref;
+            float t;
+            if (sp < kSmemStack) { int2 e = sstack[sp * stride]; ref = e.x; t = __int_as_float(e.y); }
+            else { ref = deep_ref[sp - kSmemStack]; t = deep_t[sp - kSmemStack]; }
+            if (t <= U) return ref;
         }
         return kSentinel;
     }
     __device__ __forceinline__ int visit(const float4* nodes, int node) {
-        const float4* nd = nodes + 4 * (int64_t)node;
-        float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
-        if (COUNT) box += 2;
-        float t0 = box_enter(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, U);
-        float t1 = box_enter(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, U);
-        int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
-        bool h0 = t0 != CUDART_INF_F && c0 != kEmpty, h1 = t1 != CUDART_INF_F && c1 != kEmpty;
-        if (h0 && h1) {
-            bool swap = t1 < t0;
-            if (sp < kStackDepth) { stack_ref[sp] = swap ? c0 : c1; stack_t[sp] = swap ? t0 : t1; ++sp; }
-            else error = true;
-            return swap ? c1 : c0;
-        }
-        if (h0) return c0;
-        if (h1) return c1;
-        return pop();
+        Hits4 h = visit4(nodes, node, r, U);
+        if (COUNT) box += 4;
+        if (h.n == 0) return pop();
+        if (h.n > 3) push(h.ref[3], h.t[3]);
+        if (h.n > 2) push(h.ref[2], h.t[2]);
+        if (h.n > 1) push(h.ref[1], h.t[1]);
+        return h.ref[0];
     }
     __device__ __forceinline__ void add_candidate(int k, float lo) {
         if (lo > U) return;
@@ -597,21 +628,47 @@ __device__ __forceinline__ int resolve_candidates(const SceneView& S, const Walk
     return k;
 }
 
+// Work distribution: the chunk list is cut into one contiguous range per SM
+// (partition = %smid mod n_parts) so that the warps of an SM trace the same
+// structure, and neighbouring regions of its ray space, at the same time and
+// share their L1.  A warp whose range is used up takes chunks from the next
+// ranges in turn.  counters[p] counts the chunks handed out from range p.
+__device__ __forceinline__ bool next_chunk(unsigned long long* counters, int n_parts, int& scan, int64_t total,
+                                           long long& chunk) {
+    for (; scan < n_parts; ++scan) {
+        unsigned smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        int p = (int)((smid + (unsigned)scan) % (unsigned)n_parts);
+        int64_t begin = total * p / n_parts, end = total * (p + 1) / n_parts;
+        if (begin >= end) continue;
+        unsigned long long t = atomicAdd(counters + p, 1ull);
+        if (begin + (int64_t)t < end) { chunk = begin + (int64_t)t; return true; }
+    }
+    return false;
+}
+
 template <bool EXACT, bool COUNT>
-__global__ void __launch_bounds__(128, 5) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
+__global__ void __launch_bounds__(128, 6) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
                                                    int chunk_rays, int resolve_batch, ehss_block_result* results,
-                                                   uint64_t* hist, uint64_t* ledger, unsigned long long* work) {
+                                                   uint64_t* hist, uint64_t* ledger, unsigned long long* work,
+                                                   int n_parts) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     WarpAcc& A = reinterpret_cast<WarpAcc*>(smem_raw)[warp];
     LaneRay& L = reinterpret_cast<LaneRay*>(smem_raw + sizeof(WarpAcc) * nwarps)[threadIdx.x];
+    int2* stack_base = reinterpret_cast<int2*>(smem_raw + sizeof(WarpAcc) * nwarps + sizeof(LaneRay) * blockDim.x);
     const unsigned lt_mask = (1u << lane) - 1u;
     Walker<EXACT, COUNT> W;
+    W.sstack = stack_base + threadIdx.x;
+    W.stride = blockDim.x;
+    int scan = 0;
     while (true) {
         long long c = 0;
-        if (lane == 0) c = (long long)atomicAdd(work, 1ull);
+        int have = 0;
+        if (lane == 0) have = next_chunk(work, n_parts, scan, total_chunks, c);
+        have = __shfl_sync(0xffffffffu, have, 0);
+        if (!have) break;
         c = __shfl_sync(0xffffffffu, c, 0);
-        if (c >= total_chunks) break;
         int bi = 0, hi = nb - 1;
         while (bi < hi) {
             int mid = (bi + hi + 1) >> 1;
@@ -823,7 +880,8 @@ int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const 
                   ehss_block_result* results, uint64_t* hist, uint64_t* ledger, unsigned long long* work,
                   cudaStream_t stream) {
     int warps = L.block_threads / 32;
-    size_t smem = sizeof(WarpAcc) * (size_t)warps + sizeof(LaneRay) * (size_t)L.block_threads;
+    size_t smem = sizeof(WarpAcc) * (size_t)warps + sizeof(LaneRay) * (size_t)L.block_threads +
+                  sizeof(int2) * kSmemStack * (size_t)L.block_threads;
     unsigned grid = (unsigned)(sm_count() * L.ctas_per_sm);
     int batch = L.resolve_batch > 0 ? L.resolve_batch : 1;
     const bool count = (L.options & EHSS_LAUNCH_COUNT_TESTS) != 0;
@@ -833,13 +891,15 @@ int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const 
     for (int exact = 1; exact >= 0; --exact) {
         if (!((mask >> (exact ? EHSS_PREC_FP64 : EHSS_PREC_FP32)) & 1)) continue;
         if (!first) {
-            int rc = cuda_status(cudaMemsetAsync(work, 0, 8, stream), "work counter reset");
+            int rc = cuda_status(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * kMaxWorkParts, stream),
+                                 "work counter reset");
             if (rc) return rc;
         }
         first = false;
+        const int n_parts = sm_count() < kMaxWorkParts ? sm_count() : kMaxWorkParts;
 #define EHSS_LAUNCH_BLOCKS(E, C) \
         k_blocks<E, C><<<grid, L.block_threads, smem, stream>>>(blocks, nb, total_chunks, L.chunk_rays, batch, \
-                                                                results, hist, ledger, work)
+                                                                results, hist, ledger, work, n_parts)
         if (exact) { if (count) EHSS_LAUNCH_BLOCKS(true, true); else EHSS_LAUNCH_BLOCKS(true, false); }
         else { if (count) EHSS_LAUNCH_BLOCKS(false, true); else EHSS_LAUNCH_BLOCKS(false, false); }
 #undef EHSS_LAUNCH_BLOCKS
