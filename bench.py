@@ -59,6 +59,8 @@ def parse():
     ap.add_argument('--structures', type=int, default=N_STRUCT)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-plain', action='store_true')
+    ap.add_argument('--no-serve', action='store_true')
+    ap.add_argument('--no-autotune', action='store_true')
     return ap.parse_args()
 
 
@@ -207,6 +209,36 @@ def traffic_per_launch():
 
 
 # ----------------------------------------------------------------------------
+# served form: Poisson arrivals, repeat blocks until rel. RMSE <= 1 %
+# ----------------------------------------------------------------------------
+def serving_measurement(duration_s=2.0, rate=200.0, seed=7):
+    from ehss_b200 import workloads as W
+    from ehss_b200.serve import CCSRequest, CCSServer, DeviceExecutor
+    reqs = W.request_stream(int(duration_s * rate), rate=rate, seed=seed)
+    base, base_r, _ = W.globule(1500, 4242)
+    ex = DeviceExecutor()
+    # warm-up (context, module, allocator) outside the measurement
+    warm = CCSServer(ex, block_log2=15, target=0.01)
+    warm.submit(CCSRequest('w', base, base_r, seed=1))
+    warm.run()
+    server = CCSServer(ex, block_log2=15, target=0.01)
+    for i, (t, kind, v, s) in enumerate(reqs):
+        if kind == 'globule':
+            c, r, _ = W.globule(v, s)
+        else:
+            c, r = W.ensemble_frame(base, v, sigma=0.3, seed=4242), base_r
+        server.submit(CCSRequest(i, c, r, seed=s % (2 ** 32), arrival=t))
+    server.t0 = server.clock()
+    done = server.run()
+    wall = server.now()
+    lat = server.latency_percentiles()
+    return {"requests": len(done), "arrival_rate_per_s": rate, "p50_latency_ms": lat['p50_ms'],
+            "p99_latency_ms": lat['p99_ms'], "structures_per_s": len(done) / wall, "rays_per_s": server.rays / wall,
+            "rounds": server.rounds, "converged": int(sum(d['converged'] for d in done.values())),
+            "block_rays": 1 << 15, "target_rel_rmse": 0.01}
+
+
+# ----------------------------------------------------------------------------
 # reference arm
 # ----------------------------------------------------------------------------
 def run_reference(args, world, rank):
@@ -274,7 +306,14 @@ def main():
             dist.barrier()
 
     structures, log2s, seeds = make_structures(args.structures, MASTER_SEED + rank)
-    bc = BatchCCS(structures, log2s, seeds, repeats=REPEATS, cap=CAP, precision='fp32')
+    launch = None
+    if not args.no_autotune:
+        from ehss_b200 import autotune
+        probe = BatchCCS(structures, log2s, seeds, repeats=REPEATS, cap=CAP, precision='fp32', graph=False)
+        probe.upload(); probe.build()
+        launch, _ = autotune.tune(probe.plan.jobs, passes=1)
+        del probe
+    bc = BatchCCS(structures, log2s, seeds, repeats=REPEATS, cap=CAP, precision='fp32', launch=launch)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
     stream = torch.cuda.current_stream()
 
@@ -348,13 +387,14 @@ def main():
             jobs = [j for j in bc.plan.jobs if j.tag[0] == s]
             plans.append(BlockPlan([BlockJob(j.scene, j.log2_rays, j.seed, cap=j.cap, precision=j.precision,
                                              tag=j.tag) for j in jobs]))
-        ws = torch.empty(bc.ws_bytes + 256, dtype=torch.uint8, device='cuda')
+        bs = bc.batch
+        ws = torch.empty(bs.ws_bytes + 256, dtype=torch.uint8, device='cuda')
         ws_ptr = (ws.data_ptr() + 255) & ~255
         sh = torch.cuda.current_stream().cuda_stream
 
         def plain_structure(s):
-            _lib.check(lib.ehss_scene_build(int(bc.n_atoms[s]), bc._xyz_ptrs[s], bc._r_ptrs[s], bc.leaf_size,
-                                            bc.scene_ptrs[s], bc._sizes[s], ws_ptr, bc.ws_bytes, sh))
+            _lib.check(lib.ehss_scene_build(int(bs.n_atoms[s]), bs._xyz_ptrs[s], bs._r_ptrs[s], bs.leaf_size,
+                                            bs.scene_ptrs[s], bs._sizes[s], ws_ptr, bs.ws_bytes, sh))
             plans[s].enqueue()
         for s in range(len(plans)):          # warm-up
             plain_structure(s)
@@ -405,6 +445,9 @@ def main():
             cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
                    "sample": f"{len(structures[::16])} of {len(structures)} structures (every 16th), 2^12 rays each, "
                              f"cap {CAP}; {rays_done} rays in {secs:.1f} s"}
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        serve = serving_measurement()
     if rank == 0:
         launches_per_step = 8   # 7 LBVH builder kernels + 1 persistent trace kernel (CUB sort kernels not counted)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -422,6 +465,7 @@ def main():
                 "ccs_rel_err_max_vs_fp64_oracle": ccs_err,
                 "grazing_queries": int(stats[_lib.STAT_GRAZING]), "fp64_fallback_queries": int(stats[_lib.STAT_FALLBACK]),
                 "queries": int(stats[_lib.STAT_QUERIES]), "own_traversal": own,
+                "served": serve, "launch": {k: int(v) for k, v in (launch or {}).items()} or None,
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line), flush=True)

@@ -46,7 +46,7 @@ class BlockResult(ct.Structure):
 
 class Launch(ct.Structure):
     _fields_ = [('block_threads', I32), ('ctas_per_sm', I32), ('chunk_rays', I32), ('resolve_batch', I32),
-                ('precisions', I32), ('options', I32)]
+                ('precisions', I32), ('options', I32), ('smem_stack', I32), ('reserved', I32)]
 
 
 _SIGNATURES = {
@@ -63,6 +63,8 @@ _SIGNATURES = {
     'ehss_source_rays': (ct.c_int, [P, ct.c_int, U64, I64, I64, P, P, P]),
     'ehss_trace': (ct.c_int, [P, I64, ct.c_int, ct.c_int, P, P, P, P, P, P, P, P, P]),
     'ehss_pa_anyhit': (ct.c_int, [P, I64, P, P, P, P, P, P]),
+    'ehss_pa_grid_workspace_bytes': (ct.c_int, [I64, ct.c_int, ct.c_int, P]),
+    'ehss_pa_grid': (ct.c_int, [P, I64, ct.c_int, U64, ct.c_int, P, P, P, P, U64, P]),
     'ehss_blocks_prepare': (ct.c_int, [P, ct.c_int, P, ct.c_int, P]),
     'ehss_blocks_workspace_bytes': (ct.c_int, [ct.c_int, P]),
     'ehss_trace_blocks': (ct.c_int, [P, ct.c_int, I64, P, P, P, I64, P, U64, P, P]),

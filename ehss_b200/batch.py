@@ -39,17 +39,16 @@ class SceneRef:
         self.ptr, self.radius, self.n_atoms, self.device = ptr, radius, n_atoms, device
 
 
-class BatchCCS:
-    def __init__(self, structures, log2_rays, seeds, repeats=3, cap=64, precision='fp32', ehss=True, pa=False,
-                 leaf_size=4, launch=None, device=None, graph=True):
+class BatchScenes:
+    """Many structures' scenes in one device allocation, built in one pass."""
+
+    def __init__(self, structures, leaf_size=4, device=None):
         lib = _lib.load()
         t = torch()
         self.device = require_cuda(device)
         S = len(structures)
         if S < 1:
             raise ValueError('at least one structure required')
-        log2s = [int(log2_rays)] * S if np.isscalar(log2_rays) else [int(x) for x in log2_rays]
-        seeds = [int(x) for x in (seeds if not np.isscalar(seeds) else [seeds] * S)]
         self.n_atoms = np.array([len(r) for _, r in structures], dtype=np.int64)
         if np.any(self.n_atoms < 1):
             raise ValueError('every structure needs at least one atom')
@@ -69,7 +68,6 @@ class BatchCCS:
             radii.append(enclosing_radius(c, r))
         self.d_xyz = t.empty(N * 3, dtype=t.float64, device=self.device)
         self.d_r = t.empty(N, dtype=t.float64, device=self.device)
-        # scene buffers carved from one allocation
         sizes = []
         for n in self.n_atoms:
             sb, wb = ct.c_uint64(), ct.c_uint64()
@@ -92,6 +90,31 @@ class BatchCCS:
         self._sizes = (ct.c_uint64 * S)(*sizes)
         self.leaf_size = int(leaf_size)
         self.scenes = [SceneRef(p, R, int(n), self.device) for p, R, n in zip(self.scene_ptrs, radii, self.n_atoms)]
+        self.h2d_bytes = (N * 3 + N) * 8
+
+    def upload(self):
+        self.d_xyz.copy_(self.h_xyz, non_blocking=True)
+        self.d_r.copy_(self.h_r, non_blocking=True)
+
+    def build(self, upload=True):
+        if upload:
+            self.upload()
+        lib = _lib.load()
+        _lib.check(lib.ehss_scenes_build(len(self.scenes), self._xyz_ptrs, self._r_ptrs, self._n, self.leaf_size,
+                                         self._scenes, self._sizes, self.ws_ptr, self.ws_bytes,
+                                         stream_handle(self.device)), 'batched scene build')
+
+
+class BatchCCS:
+    def __init__(self, structures, log2_rays, seeds, repeats=3, cap=64, precision='fp32', ehss=True, pa=False,
+                 leaf_size=4, launch=None, device=None, graph=True):
+        S = len(structures)
+        log2s = [int(log2_rays)] * S if np.isscalar(log2_rays) else [int(x) for x in log2_rays]
+        seeds = [int(x) for x in (seeds if not np.isscalar(seeds) else [seeds] * S)]
+        self.batch = BatchScenes(structures, leaf_size=leaf_size, device=device)
+        self.device = self.batch.device
+        self.scenes = self.batch.scenes
+        self.n_atoms = self.batch.n_atoms
         prec = {'fp64': _lib.PREC_FP64, 'fp32': _lib.PREC_FP32}[precision] if isinstance(precision, str) else precision
         jobs = []
         for s, (sc, lg, sd) in enumerate(zip(self.scenes, log2s, seeds)):
@@ -101,19 +124,15 @@ class BatchCCS:
         self.plan = BlockPlan(jobs, launch=launch, device=self.device)
         self.rays = self.plan.rays
         self.use_graph = graph
-        self.h2d_bytes = (N * 3 + N) * 8
+        self.h2d_bytes = self.batch.h2d_bytes
         self.d2h_bytes = self.plan.results.numel() + 16 * self.plan.hist.numel()
 
     # -- stages ---------------------------------------------------------------
     def upload(self):
-        self.d_xyz.copy_(self.h_xyz, non_blocking=True)
-        self.d_r.copy_(self.h_r, non_blocking=True)
+        self.batch.upload()
 
     def build(self):
-        lib = _lib.load()
-        _lib.check(lib.ehss_scenes_build(len(self.scenes), self._xyz_ptrs, self._r_ptrs, self._n, self.leaf_size,
-                                         self._scenes, self._sizes, self.ws_ptr, self.ws_bytes,
-                                         stream_handle(self.device)), 'batched scene build')
+        self.batch.build(upload=False)
 
     def trace(self):
         if self.use_graph and self.plan.graph is None:

@@ -24,7 +24,8 @@ import numpy as np
 from . import _lib
 from .device import empty, ptr, stream_handle, torch
 
-DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=6, chunk_rays=256, resolve_batch=24, count_tests=False)
+DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=6, chunk_rays=256, resolve_batch=24, smem_stack=16,
+                      count_tests=False)
 
 
 @dataclass
@@ -54,7 +55,7 @@ class BlockPlan:
             precisions |= 1 << int(j.precision)
         self.launch = _lib.Launch(int(L['block_threads']), int(L['ctas_per_sm']), int(L['chunk_rays']),
                                   int(L['resolve_batch']), precisions,
-                                  _lib.LAUNCH_COUNT_TESTS if L['count_tests'] else 0)
+                                  _lib.LAUNCH_COUNT_TESTS if L['count_tests'] else 0, int(L['smem_stack']), 0)
         n = len(self.jobs)
         host = (_lib.Block * n)()
         seeds = (ct.c_uint64 * n)()

@@ -191,6 +191,30 @@ int ehss_pa_anyhit(const void* scene_dev, int64_t n_rays, const double* origins_
                           as_stream(stream));
 }
 
+static bool pow2_in(int64_t v, int64_t lo, int64_t hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
+
+int ehss_pa_grid_workspace_bytes(int64_t n_atoms, int n_dirs, int n, uint64_t* bytes) {
+    clear_error();
+    if (!bytes || n_atoms < 1 || !pow2_in(n_dirs, 1, 1 << 16) || !pow2_in(n, 8, 8192)) {
+        set_error("need n_atoms >= 1, n_dirs a power of two in 1..65536 and n a power of two in 8..8192");
+        return EHSS_ERR_VALUE;
+    }
+    *bytes = grid_workspace_bytes(n_atoms, n_dirs, n);
+    return EHSS_OK;
+}
+
+int ehss_pa_grid(const void* scene_dev, int64_t n_atoms, int n_dirs, uint64_t seed, int n, uint64_t* counts_dev,
+                 double* spacing_dev, double* xy_dev, void* workspace_dev, uint64_t workspace_bytes, void* stream) {
+    clear_error();
+    if (!scene_dev || !counts_dev || !workspace_dev) { set_error("null pointer"); return EHSS_ERR_VALUE; }
+    if (n_atoms < 1 || !pow2_in(n_dirs, 1, 1 << 16) || !pow2_in(n, 8, 8192)) {
+        set_error("need n_atoms >= 1, n_dirs a power of two in 1..65536 and n a power of two in 8..8192");
+        return EHSS_ERR_VALUE;
+    }
+    return launch_grid_pa(scene_dev, n_atoms, n_dirs, seed, n, reinterpret_cast<unsigned long long*>(counts_dev),
+                          spacing_dev, xy_dev, workspace_dev, workspace_bytes, as_stream(stream));
+}
+
 int ehss_blocks_prepare(ehss_block* blocks, int n_blocks, const uint64_t* seeds, int chunk_rays, int64_t* total_chunks) {
     clear_error();
     if (!blocks || !seeds || !total_chunks || n_blocks < 1) { set_error("invalid arguments"); return EHSS_ERR_VALUE; }
@@ -243,11 +267,12 @@ int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_
         return EHSS_ERR_CAPACITY;
     }
     const ehss_launch& L = *launch;
-    if (L.block_threads != 128) {
-        set_error("block_threads must be 128");
+    if (L.smem_stack < 0 || L.smem_stack > 32) { set_error("smem_stack must be 0..32"); return EHSS_ERR_VALUE; }
+    if (L.block_threads != 64 && L.block_threads != 128) {
+        set_error("block_threads must be 64 or 128");
         return EHSS_ERR_VALUE;
     }
-    if (L.ctas_per_sm < 1 || L.ctas_per_sm > 32) { set_error("ctas_per_sm must be 1..32"); return EHSS_ERR_VALUE; }
+    if (L.ctas_per_sm < 1 || L.ctas_per_sm > 16) { set_error("ctas_per_sm must be 1..16"); return EHSS_ERR_VALUE; }
     if (L.chunk_rays < 32 || L.chunk_rays > 4096 || (L.chunk_rays & (L.chunk_rays - 1))) {
         set_error("chunk_rays must be a power of two in 32..4096");
         return EHSS_ERR_VALUE;

@@ -235,6 +235,9 @@ int launch_pa_rays(const void* scene, int64_t n, const double* P, const double* 
 int launch_sobol_points(int dim, const SobolParams& p, int64_t first, int64_t n, uint32_t* q, cudaStream_t stream);
 int launch_source_rays(const void* scene, const Sobol4Params& p, int64_t first, int64_t n, double* O, double* D,
                        cudaStream_t stream);
+uint64_t grid_workspace_bytes(int64_t n_atoms, int n_dirs, int n);
+int launch_grid_pa(const void* scene, int64_t n_atoms, int n_dirs, uint64_t seed, int n, unsigned long long* counts,
+                   double* spacing_out, double* xy_out, void* workspace, uint64_t ws_bytes, cudaStream_t stream);
 int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const ehss_launch& L,
                   ehss_block_result* results, uint64_t* hist, uint64_t* ledger, unsigned long long* work,
                   cudaStream_t stream);

@@ -502,7 +502,7 @@ constexpr int kNoLeaf = INT32_MAX;
 // memory (entry i of lane t at smem_stack[i * blockDim + t], conflict-free);
 // deeper entries, rare for an LBVH walked near-child first, go to a
 // per-lane local array.
-constexpr int kSmemStack = 16;
+constexpr int kSmemStackMax = 32;
 
 template <bool EXACT, bool COUNT>
 struct Walker {
@@ -517,12 +517,13 @@ struct Walker {
     unsigned box, sphere;
     int2* sstack;          // this lane's shared-memory stack column
     int stride;            // entries are stride apart (blockDim.x)
-    int deep_ref[kStackDepth - kSmemStack];
-    float deep_t[kStackDepth - kSmemStack];
+    int sdepth;            // entries kept in shared memory (launch parameter)
+    int deep_ref[kStackDepth];
+    float deep_t[kStackDepth];
 
     __device__ __forceinline__ void push(int ref, float t) {
-        if (sp < kSmemStack) sstack[sp * stride] = make_int2(ref, __float_as_int(t));
-        else if (sp < kStackDepth) { deep_ref[sp - kSmemStack] = ref; deep_t[sp - kSmemStack] = t; }
+        if (sp < sdepth) sstack[sp * stride] = make_int2(ref, __float_as_int(t));
+        else if (sp < kStackDepth) { deep_ref[sp - sdepth] = ref; deep_t[sp - sdepth] = t; }
         else { error = true; return; }
         ++sp;
     }
@@ -540,8 +541,8 @@ struct Walker {
             --sp;
             int ref;
             float t;
-            if (sp < kSmemStack) { int2 e = sstack[sp * stride]; ref = e.x; t = __int_as_float(e.y); }
-            else { ref = deep_ref[sp - kSmemStack]; t = deep_t[sp - kSmemStack]; }
+            if (sp < sdepth) { int2 e = sstack[sp * stride]; ref = e.x; t = __int_as_float(e.y); }
+            else { ref = deep_ref[sp - sdepth]; t = deep_t[sp - sdepth]; }
             if (t <= U) return ref;
         }
         return kSentinel;
@@ -651,7 +652,7 @@ template <bool EXACT, bool COUNT>
 __global__ void __launch_bounds__(128, 6) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
                                                    int chunk_rays, int resolve_batch, ehss_block_result* results,
                                                    uint64_t* hist, uint64_t* ledger, unsigned long long* work,
-                                                   int n_parts) {
+                                                   int n_parts, int smem_stack) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     WarpAcc& A = reinterpret_cast<WarpAcc*>(smem_raw)[warp];
@@ -661,6 +662,7 @@ __global__ void __launch_bounds__(128, 6) k_blocks(const ehss_block* blocks, int
     Walker<EXACT, COUNT> W;
     W.sstack = stack_base + threadIdx.x;
     W.stride = blockDim.x;
+    W.sdepth = smem_stack;
     int scan = 0;
     while (true) {
         long long c = 0;
@@ -880,8 +882,9 @@ int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const 
                   ehss_block_result* results, uint64_t* hist, uint64_t* ledger, unsigned long long* work,
                   cudaStream_t stream) {
     int warps = L.block_threads / 32;
+    const int sdepth = L.smem_stack > 0 ? L.smem_stack : 16;
     size_t smem = sizeof(WarpAcc) * (size_t)warps + sizeof(LaneRay) * (size_t)L.block_threads +
-                  sizeof(int2) * kSmemStack * (size_t)L.block_threads;
+                  sizeof(int2) * sdepth * (size_t)L.block_threads;
     unsigned grid = (unsigned)(sm_count() * L.ctas_per_sm);
     int batch = L.resolve_batch > 0 ? L.resolve_batch : 1;
     const bool count = (L.options & EHSS_LAUNCH_COUNT_TESTS) != 0;
@@ -899,7 +902,7 @@ int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const 
         const int n_parts = sm_count() < kMaxWorkParts ? sm_count() : kMaxWorkParts;
 #define EHSS_LAUNCH_BLOCKS(E, C) \
         k_blocks<E, C><<<grid, L.block_threads, smem, stream>>>(blocks, nb, total_chunks, L.chunk_rays, batch, \
-                                                                results, hist, ledger, work, n_parts)
+                                                                results, hist, ledger, work, n_parts, sdepth)
         if (exact) { if (count) EHSS_LAUNCH_BLOCKS(true, true); else EHSS_LAUNCH_BLOCKS(true, false); }
         else { if (count) EHSS_LAUNCH_BLOCKS(false, true); else EHSS_LAUNCH_BLOCKS(false, false); }
 #undef EHSS_LAUNCH_BLOCKS

@@ -157,6 +157,21 @@ int ehss_pa_anyhit(const void* scene_dev, int64_t n_rays, const double* origins_
                    const int64_t* owners_dev, uint8_t* blocked_dev, uint64_t* stats_dev, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Adaptive finite-grid PA.  Replaces ccs_cli.adaptive_pa (ccs_cli.py:142-160)
+ * with project_grid (pa_walsh_geometry.py:171-180) and the sparse quadtree
+ * count block_disks/block_count (pa_sparse_blocks.py:134-166): for direction
+ * k of the n_dirs Sobol(2, seed) directions, counts_dev[k] receives the
+ * number of pixels of the n x n midpoint grid covered by the union of the
+ * projected atom disks (row_span's exact inequality, pa_dyadic_bitmask.py:
+ * 50-61) and spacing_dev[k] (or NULL) the pixel size; the direction's area is
+ * counts * spacing^2 and the PA is their mean.  xy_dev (NULL or float64
+ * [n_dirs * n_atoms * 2]) receives the projected centres.  n_atoms must be
+ * the scene's atom count; n_dirs and n are powers of two. */
+int ehss_pa_grid_workspace_bytes(int64_t n_atoms, int n_dirs, int n, uint64_t* workspace_bytes);
+int ehss_pa_grid(const void* scene_dev, int64_t n_atoms, int n_dirs, uint64_t seed, int n, uint64_t* counts_dev,
+                 double* spacing_dev, double* xy_dev, void* workspace_dev, uint64_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Fused blocks: Sobol -> impact disk -> trace -> (1 - cos chi) reduction,
  * with no per-ray HBM traffic.  One block = one replicate of one structure
  * (the body of ccs_cli.solve_frame's repeat loop, ccs_cli.py:189-219).  The
@@ -213,7 +228,7 @@ int ehss_blocks_workspace_bytes(int n_blocks, uint64_t* bytes);
 
 /* Launch configuration chosen by the caller or the autotuner. */
 typedef struct ehss_launch {
-    int32_t block_threads;    /* 64..256, multiple of 32 */
+    int32_t block_threads;    /* 64 or 128 */
     int32_t ctas_per_sm;      /* persistent CTAs per SM (grid = SMs * ctas_per_sm) */
     int32_t chunk_rays;       /* rays per work item (as passed to ehss_blocks_prepare) */
     int32_t resolve_batch;    /* a warp leaves its traversal phase once this many lanes have a
@@ -221,6 +236,9 @@ typedef struct ehss_launch {
     int32_t precisions;       /* bit mask of the EHSS_PREC_* values present among the blocks
                                  (1 << EHSS_PREC_FP64 | 1 << EHSS_PREC_FP32); 0 = both */
     int32_t options;          /* EHSS_LAUNCH_* bits */
+    int32_t smem_stack;       /* traversal-stack entries per lane kept in shared memory
+                                 (0 = 16, max 32); deeper entries go to local memory */
+    int32_t reserved;         /* 0 */
 } ehss_launch;
 #define EHSS_LAUNCH_COUNT_TESTS 1   /* count box and sphere tests into the block stats (slower) */
 

@@ -456,3 +456,59 @@ void oracle_pa_blocked(int64_t nr, const double* origins, const double* dirs, co
     (void)nn;
     counters[0] = boxes; counters[1] = tests;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Adaptive finite-grid PA.                                                */
+/* ---------------------------------------------------------------------- */
+
+/* row_span (pa_dyadic_bitmask.py:50-61): covered pixels [lo, hi) of row y
+ * for the disk (cx, cy, r); pixel i has midpoint lower + (i + 0.5) spacing and
+ * is covered when (x_mid - cx)^2 <= r^2 - (y_mid - cy)^2. */
+static void row_span(double cx, double cy, double r, double lower0, double lower1, double spacing, int64_t y,
+                     int64_t n, int64_t* lo_out, int64_t* hi_out) {
+    double dy = lower1 + (y + .5) * spacing - cy;
+    double rem = r * r - dy * dy;
+    *lo_out = 0; *hi_out = 0;
+    if (rem < 0) return;
+    double half = sqrt(rem);
+    double a = ceil((cx - half - lower0) / spacing - .5);
+    double b = floor((cx + half - lower0) / spacing - .5);
+    int64_t lo = (int64_t)a, hi = (int64_t)b + 1;
+    lo = lo < n ? lo : n; lo = lo > 0 ? lo : 0;
+    hi = hi < n ? hi : n; hi = hi > 0 ? hi : 0;
+    while (lo > 0) { double t = lower0 + (lo - .5) * spacing - cx; if (t * t <= rem) lo -= 1; else break; }
+    while (lo < hi) { double t = lower0 + (lo + .5) * spacing - cx; if (t * t > rem) lo += 1; else break; }
+    while (hi < n) { double t = lower0 + (hi + .5) * spacing - cx; if (t * t <= rem) hi += 1; else break; }
+    while (hi > lo) { double t = lower0 + (hi - .5) * spacing - cx; if (t * t > rem) hi -= 1; else break; }
+    *lo_out = lo; *hi_out = hi;
+}
+
+/* row_bounds (pa_dyadic_bitmask.py:63-68). */
+static void row_bounds(double cy, double r, double lower1, double spacing, int64_t n, int64_t* lo, int64_t* hi) {
+    int64_t a = (int64_t)ceil((cy - r - lower1) / spacing - .5) - 1;
+    int64_t b = (int64_t)floor((cy + r - lower1) / spacing - .5) + 2;
+    a = a < n ? a : n; a = a > 0 ? a : 0;
+    b = b < n ? b : n; b = b > 0 ? b : 0;
+    *lo = a; *hi = b;
+}
+
+/* Pixels of the n x n midpoint grid covered by the union of the disks
+ * (the quantity block_count(block_disks(...)) counts, pa_sparse_blocks.py:134-166);
+ * bits: caller-provided n*ceil(n/64) uint64 words. */
+int64_t oracle_union_count(int64_t m, const double* xy, const double* radii, double lower0, double lower1,
+                           double spacing, int64_t n, uint64_t* bits) {
+    int64_t words = (n + 63) / 64;
+    memset(bits, 0, sizeof(uint64_t) * (size_t)(n * words));
+    for (int64_t a = 0; a < m; ++a) {
+        int64_t y0, y1;
+        row_bounds(xy[2 * a + 1], radii[a], lower1, spacing, n, &y0, &y1);
+        for (int64_t y = y0; y < y1; ++y) {
+            int64_t lo, hi;
+            row_span(xy[2 * a], xy[2 * a + 1], radii[a], lower0, lower1, spacing, y, n, &lo, &hi);
+            for (int64_t x = lo; x < hi; ++x) bits[y * words + x / 64] |= (uint64_t)1 << (x % 64);
+        }
+    }
+    int64_t count = 0;
+    for (int64_t i = 0; i < n * words; ++i) count += __builtin_popcountll(bits[i]);
+    return count;
+}

@@ -189,6 +189,8 @@ def lib():
         L.oracle_sphere_hit.argtypes = [P, P, P, ct.c_double]
         L.oracle_pa_tree.restype = I64
         L.oracle_pa_tree.argtypes = [I64, P, P, I64] + [P] * 6
+        L.oracle_union_count.restype = I64
+        L.oracle_union_count.argtypes = [I64, P, P, ct.c_double, ct.c_double, ct.c_double, I64, P]
         L.oracle_pa_blocked.restype = None
         L.oracle_pa_blocked.argtypes = [I64, P, P, P, P, P, I64] + [P] * 6 + [P, P, ct.c_int]
         _LIB = L
@@ -367,3 +369,41 @@ def summarize(values):
 
 def host_cores():
     return len(os.sched_getaffinity(0)) if hasattr(os, 'sched_getaffinity') else (os.cpu_count() or 1)
+
+
+# --------------------------------------------------------------------------
+# Adaptive finite-grid PA (ccs_cli.adaptive_pa, ccs_cli.py:142-160;
+# project_grid, pa_walsh_geometry.py:171-180)
+# --------------------------------------------------------------------------
+def pa_directions(n_dirs, seed):
+    return unit_sphere(sobol_points(2, int(n_dirs).bit_length() - 1, seed))
+
+
+def project_grid(centers, radii, direction, n):
+    direction = np.asarray(direction, float)
+    direction = direction / np.linalg.norm(direction)
+    axis = np.array([0., 0., 1.]) if abs(direction[2]) < .9 else np.array([1., 0., 0.])
+    u = np.cross(axis, direction); u /= np.linalg.norm(u); v = np.cross(direction, u)
+    centered = centers - centers.mean(axis=0)
+    xy = np.column_stack((centered @ u, centered @ v))
+    extent = float(np.max(np.abs(xy) + radii[:, None])) * (1. + 1e-10)
+    lower = np.array([-extent, -extent]); spacing = 2 * extent / n
+    return xy, lower, spacing
+
+
+def union_count(xy, radii, lower, spacing, n):
+    xy = _c(xy, np.float64); radii = _c(radii, np.float64)
+    bits = np.zeros(int(n) * ((int(n) + 63) // 64), dtype=np.uint64)
+    return int(lib().oracle_union_count(len(radii), _p(xy), _p(radii), float(lower[0]), float(lower[1]),
+                                        float(spacing), int(n), _p(bits)))
+
+
+def adaptive_pa(centers, radii, n_dirs, grid, seed):
+    centers = _c(centers, np.float64); radii = _c(radii, np.float64)
+    counts, spacings, values = [], [], []
+    for d in pa_directions(n_dirs, seed):
+        xy, lower, spacing = project_grid(centers, radii, d, grid)
+        c = union_count(xy, radii, lower, spacing, grid)
+        counts.append(c); spacings.append(spacing)
+        values.append(float(c) * spacing ** 2)
+    return dict(pa_angstrom2=float(np.mean(values)), counts=counts, spacings=spacings, values=values)

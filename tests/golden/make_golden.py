@@ -166,6 +166,26 @@ def main():
             pa[f'{name}_tree_{key}'] = getattr(idx.tree, key)
     np.savez_compressed(HERE / 'pa.npz', **pa)
 
+    # ---- adaptive finite-grid PA ---------------------------------------------------
+    from support_exchange_transport.pa_walsh_geometry import project_grid
+    from support_exchange_transport.pa_sparse_blocks import block_disks, block_count
+    from support_exchange_transport.inside_out_pa import unit_sphere
+    ada = {}
+    for name, s, ndir, grid, seed in [('cloud37', c37, 8, 128, 5), ('cloud300', g300, 16, 256, 190003),
+                                      ('tri', tri, 8, 512, 0), ('single', Spheres(np.zeros((1, 3)), [3.1]), 4, 64, 2)]:
+        ds = unit_sphere(qmc.Sobol(2, scramble=True, seed=seed).random_base2(ndir.bit_length() - 1))
+        counts, spacings, xys = [], [], []
+        for d in ds:
+            xy, lower, spacing, *_ = project_grid(s, d, grid)
+            full, partial, _ = block_disks(xy, s.radii, lower, spacing, grid)
+            counts.append(int(block_count(full, partial))); spacings.append(spacing); xys.append(xy)
+        out = ccs_cli.adaptive_pa(s, ndir, grid, seed)
+        ada[name + '_centers'] = s.centers; ada[name + '_radii'] = s.radii
+        ada[name + '_args'] = np.array([ndir, grid, seed])
+        ada[name + '_counts'] = np.array(counts); ada[name + '_spacings'] = np.array(spacings)
+        ada[name + '_xy'] = np.array(xys); ada[name + '_pa'] = np.array(out['pa_angstrom2'])
+    np.savez_compressed(HERE / 'pa_adaptive.npz', **ada)
+
     # ---- CLI solve_frame readouts ------------------------------------------------
     cli = {}
 
@@ -179,7 +199,8 @@ def main():
     for name, s, extra in [
             ('single', Spheres(np.zeros((1, 3)), np.array([3.1])), ['--pa-method', 'bvh']),
             ('cap1', c23, ['--pa-method', 'bvh', '--repeats', '1', '--max-collisions', '1']),
-            ('tri', tri, ['--pa-method', 'bvh', '--rays', '4096', '--repeats', '3', '--seed', '0'])]:
+            ('tri', tri, ['--pa-method', 'bvh', '--rays', '4096', '--repeats', '3', '--seed', '0']),
+            ('tri_adaptive', tri, ['--directions', '16', '--grid-size', '256', '--repeats', '2'])]:
         argv = ['unused.xyz', '--rays', '1024', '--repeats', '2', '--output', '/nonexistent/x', *extra]
         a = ccs_cli.parser().parse_args(argv)
         out = ccs_cli.solve_frame(s, a, False)

@@ -301,3 +301,65 @@ def test_invalid_inputs_raise(eb):
         eng.trace(bad, 4)
     with pytest.raises(ValueError):
         eb.PreparedStaticGPUEHSS(Spheres([[0, 0, 0], [2, 0, 0]], [1, 1]), groups=[0, 2])
+
+
+@pytest.mark.parametrize('name', ['cloud37', 'cloud300', 'tri', 'single'])
+def test_adaptive_pa_counts_exact_and_pa_close(eb, golden, name):
+    from ehss_b200.adaptive_pa import adaptive_pa, grid_counts
+    g = golden('pa_adaptive.npz')
+    ndir, grid, seed = (int(x) for x in g[name + '_args'])
+    c, r = g[name + '_centers'], g[name + '_radii']
+    scene = eb.Scene(c, r)
+    counts, spacing, xy = grid_counts(scene, ndir, grid, seed, with_xy=True)
+    for k in range(ndir):      # identical projected coordinates -> identical integer counts
+        lower = np.array([-spacing[k] * grid / 2] * 2)
+        assert counts[k] == O.union_count(xy[k], r, lower, spacing[k], grid), k
+    np.testing.assert_allclose(spacing, g[name + '_spacings'], rtol=1e-14)
+    np.testing.assert_allclose(xy, g[name + '_xy'], rtol=0, atol=1e-12 * (1 + np.abs(c).max()))
+    # against the reference's own value: boundary pixels may flip with ulp-level projection differences
+    got = adaptive_pa(eb.Spheres(c, r, deduplicate=False), ndir, grid, seed, scene=scene)['pa_angstrom2']
+    assert got == pytest.approx(float(g[name + '_pa']), rel=4.0 / grid ** 2)
+
+
+def test_cli_end_to_end(eb, tmp_path):
+    """ccs.py surface on the device against the reference's solve_frame readouts."""
+    import csv
+    import json
+    from ehss_b200 import ccs_cli
+    from tests.conftest import GOLDEN
+    cli = json.loads((GOLDEN / 'cli.json').read_text())
+    for name, case in cli.items():
+        argv = [a for a in case['argv'] if a not in ('unused.xyz',)]
+        argv[argv.index('--output') + 1] = str(tmp_path / name)
+        spheres = eb.Spheres(np.array(case['centers']), np.array(case['radii']), deduplicate=False)
+        args = ccs_cli.parser().parse_args(['x.xyz'] + argv)
+        out = ccs_cli.solve_frame(spheres, args, progress=False)
+        ref = case['summary']
+        if 'ehss_angstrom2' in ref:
+            assert out['summary']['ehss_angstrom2']['mean'] == pytest.approx(ref['ehss_angstrom2']['mean'], rel=1e-12)
+            assert out['summary']['ehss_tail_bound_mean_angstrom2'] == pytest.approx(
+                ref['ehss_tail_bound_mean_angstrom2'], rel=1e-12, abs=1e-12)
+            for a, b in zip(out['runs'], case['runs']):
+                assert a['seed'] == b['seed']
+                assert a['ehss']['collision_histogram'] == b['ehss']['collision_histogram']
+                assert a['ehss']['unresolved_rays'] == b['ehss']['unresolved_rays']
+        if 'pa_angstrom2' in ref:
+            grid = args.grid_size
+            tol = 1e-12 if args.pa_method == 'bvh' else 4.0 / grid ** 2
+            assert out['summary']['pa_angstrom2']['mean'] == pytest.approx(ref['pa_angstrom2']['mean'], rel=tol)
+    # the full command line on an XYZ file writes the reference's two output files
+    xyz = tmp_path / 'water.xyz'
+    xyz.write_text('3\nwater\nO 0 0 0\nH 0.9572 0 0\nH -0.239987 0.926627 0\n')
+    outdir = tmp_path / 'run'
+    assert ccs_cli.main([str(xyz), '--rays', '1024', '--directions', '8', '--grid-size', '128', '--repeats', '2',
+                         '--output', str(outdir)]) == 0
+    payload = json.loads((outdir / 'results.json').read_text())
+    assert payload['schema_version'] == 1 and len(payload['records']) == 1
+    rec = payload['records'][0]
+    assert set(rec['summary']) >= {'pa_angstrom2', 'ehss_angstrom2', 'ehss_tail_bound_mean_angstrom2'}
+    with (outdir / 'summary.csv').open(encoding='utf-8-sig', newline='') as f:
+        rows = list(csv.DictReader(f))
+    assert len(rows) == 1 and float(rows[0]['ehss_mean_A2']) > 0
+    with pytest.raises(SystemExit) as e:
+        ccs_cli.main([str(xyz), '--rays', '1000', '--output', str(tmp_path / 'bad')])
+    assert e.value.code == 2

@@ -86,7 +86,7 @@ def test_struct_layouts_match_header():
     from ehss_b200 import _lib
     assert ct.sizeof(_lib.Block) == 544 and _lib.Block.basis.offset == 0 and _lib.Block.base.offset == 480
     assert ct.sizeof(_lib.BlockResult) == 8 * (5 + _lib.NSTATS)
-    assert ct.sizeof(_lib.Launch) == 24
+    assert ct.sizeof(_lib.Launch) == 32
 
 
 def test_workload_generators():

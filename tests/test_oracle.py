@@ -137,6 +137,7 @@ def test_cli_readout_matches_reference_solve_frame():
         seed, cap = flag('--seed', 190003), flag('--max-collisions', 64)
         centers, radii = np.array(case['centers']), np.array(case['radii'])
         tree = O.StaticTree(centers, radii, 4); pat = O.PATree(centers, radii, 4)
+        adaptive = '--pa-method' not in argv or argv[argv.index('--pa-method') + 1] == 'adaptive'
         omegas = []
         for k in range(repeats):
             s = (seed + 104729 * k) % 2 ** 32
@@ -148,7 +149,24 @@ def test_cli_readout_matches_reference_solve_frame():
             for key in ('ehss_angstrom2', 'pa_from_same_rays_angstrom2', 'tail_bound_angstrom2', 'unresolved_rays',
                         'collision_histogram', 'collision_contribution_angstrom2'):
                 assert ro[key] == run['ehss'][key], (name, k, key)
-            hits, _, _ = pat.query(src['origins'], src['directions'])
-            assert float(src['weights'][hits].sum()) == run['pa']['pa_angstrom2']
+            if adaptive:
+                ada = O.adaptive_pa(centers, radii, flag('--directions', 64), flag('--grid-size', 512), s)
+                assert ada['pa_angstrom2'] == run['pa']['pa_angstrom2']
+            else:
+                hits, _, _ = pat.query(src['origins'], src['directions'])
+                assert float(src['weights'][hits].sum()) == run['pa']['pa_angstrom2']
             omegas.append(ro['ehss_angstrom2'])
         assert O.summarize(omegas) == case['summary']['ehss_angstrom2']
+
+
+@pytest.mark.parametrize('name', ['cloud37', 'cloud300', 'tri', 'single'])
+def test_adaptive_pa_bit_exact(golden, name):
+    g = golden('pa_adaptive.npz')
+    ndir, grid, seed = (int(x) for x in g[name + '_args'])
+    r = O.adaptive_pa(g[name + '_centers'], g[name + '_radii'], ndir, grid, seed)
+    assert r['counts'] == g[name + '_counts'].tolist()
+    assert r['spacings'] == g[name + '_spacings'].tolist()
+    assert r['pa_angstrom2'] == float(g[name + '_pa'])
+    # the union count from the reference's own projected coordinates
+    for xy, sp, c in zip(g[name + '_xy'], g[name + '_spacings'], g[name + '_counts']):
+        assert O.union_count(xy, g[name + '_radii'], np.array([-sp * grid / 2] * 2), sp, grid) == c

@@ -1,0 +1,154 @@
+"""Host logic of the served form and of the multi-GPU sharding (CPU only).
+
+The server's device side is replaced by a fake executor whose block results
+are a deterministic function of (structure, seed), like the device's integer
+sums; the sharded path runs as two gloo ranks on CPU.
+"""
+import math
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from ehss_b200.serve import CCSRequest, CCSServer, rel_rmse
+from ehss_b200 import distributed as D
+
+
+class FakeExecutor:
+    """Block value = structure-dependent mean + seeded noise; 100 bytes per atom."""
+
+    def __init__(self, noise=0.02):
+        self.noise = noise
+        self.built, self.released, self.traced = [], [], []
+
+    def footprint(self, n_atoms):
+        return 100 * n_atoms
+
+    def build(self, structures):
+        handles = []
+        for c, r in structures:
+            h = (len(r), float(np.round(c.sum(), 6)))
+            self.built.append(h)
+            handles.append(h)
+        return handles
+
+    def trace(self, jobs):
+        self.traced.append(len(jobs))
+        out = []
+        for (n, key), log2, seed in jobs:
+            rng = np.random.default_rng([n, int(abs(key) * 1000) % 2 ** 31, seed])
+            out.append((100.0 + n + self.noise * (100 + n) * rng.normal(), 0.0))
+        return out
+
+    def release(self, handle):
+        self.released.append(handle)
+
+
+def _req(rid, n, seed=1, arrival=0.0):
+    rng = np.random.default_rng(n)
+    return CCSRequest(rid, rng.normal(size=(n, 3)), np.ones(n), seed=seed, arrival=arrival)
+
+
+def test_rel_rmse():
+    assert math.isinf(rel_rmse([1.0]))
+    a = [1.0, 1.1, 0.9, 1.0]
+    assert rel_rmse(a) == pytest.approx(np.std(a, ddof=1) / 2 / 1.0)
+
+
+def test_results_same_alone_and_in_the_mix():
+    alone = CCSServer(FakeExecutor(), target=0.01)
+    alone.submit(_req('a', 50, seed=7))
+    ra = alone.run()['a']
+    mixed = CCSServer(FakeExecutor(), target=0.01)
+    for rid, n, seed in [('b', 300, 3), ('a', 50, 7), ('c', 12, 9), ('d', 1000, 11)]:
+        mixed.submit(_req(rid, n, seed=seed))
+    rm = mixed.run()['a']
+    assert ra['values'] == rm['values'] and ra['blocks'] == rm['blocks']
+    assert rm['converged'] and rm['rel_rmse'] <= 0.01 and rm['blocks'] >= 2
+
+
+def test_admission_by_memory_and_rejection():
+    ex = FakeExecutor()
+    server = CCSServer(ex, budget_bytes=100 * 1500, target=0.01)
+    server.submit(_req('big', 1000))
+    server.submit(_req('big2', 1000))       # does not fit beside 'big'
+    server.submit(_req('small', 100))
+    server.step()
+    assert {s.req.rid for s in server.active} | set(server.done) == {'big', 'small'}
+    assert [s.req.rid for s in server.pending] == ['big2']
+    done = server.run()
+    assert set(done) == {'big', 'big2', 'small'}
+    assert done['big2']['admitted_s'] >= done['big']['latency_s'] - 1e-9   # waited for memory
+    assert server.used == 0 and len(ex.released) == 3
+    with pytest.raises(ValueError):
+        server.submit(_req('huge', 5000))
+
+
+def test_late_arrivals_join_running_rounds():
+    t = [0.0]
+    ex = FakeExecutor(noise=0.05)
+    server = CCSServer(ex, target=0.01, clock=lambda: t[0])
+    server.submit(_req('early', 40, arrival=0.0))
+    server.submit(_req('late', 60, arrival=0.5))
+    server.step()
+    assert [s.req.rid for s in server.active] == ['early']
+    t[0] = 0.6
+    server.step()
+    rids = {s.req.rid for s in server.active} | set(server.done)
+    assert 'late' in rids and 'early' in rids
+    while server.active or server.pending:
+        t[0] += 0.01
+        server.step()
+    assert server.done['late']['latency_s'] > 0
+
+
+def test_shard_balances_and_covers():
+    costs = [D.estimated_cost(n, 1 << lg) for n, lg in [(20, 14), (5000, 18), (300, 16), (40, 15), (1200, 17)]]
+    owner = D.shard(costs, 2)
+    assert sorted(set(owner)) == [0, 1]
+    loads = [sum(c for c, o in zip(costs, owner) if o == r) for r in (0, 1)]
+    assert max(loads) - min(loads) <= max(costs)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(('127.0.0.1', 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, structures, log2s, seeds, out):
+    import torch.distributed as dist
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        def run_local(indices):
+            return {i: dict(structure=i, value=float(len(structures[i][1]) * 2 + seeds[i])) for i in indices}
+        res = D.run_sharded(structures, log2s, seeds, run_local, rank, world)
+        if rank == 0:
+            out.put(res)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_gather_with_two_gloo_ranks():
+    import torch.multiprocessing as mp
+    structures = [(np.zeros((n, 3)), np.ones(n)) for n in (20, 300, 5000, 45, 1200, 7)]
+    log2s = [14, 15, 18, 14, 17, 14]
+    seeds = list(range(len(structures)))
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, structures, log2s, seeds, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert [r['structure'] for r in res] == list(range(len(structures)))
+    assert [r['value'] for r in res] == [float(len(s[1]) * 2 + i) for i, s in enumerate(structures)]
