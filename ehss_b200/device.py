@@ -14,8 +14,9 @@ def require_cuda(device=None):
     t = torch()
     if not t.cuda.is_available():
         raise RuntimeError('ehss_b200 needs a CUDA device (B200, sm_100a); none is available')
-    dev = t.device('cuda', t.cuda.current_device() if device is None else int(device))
-    return dev
+    if isinstance(device, t.device):
+        return device if device.index is not None else t.device('cuda', t.cuda.current_device())
+    return t.device('cuda', t.cuda.current_device() if device is None else int(device))
 
 
 def stream_handle(device=None):
