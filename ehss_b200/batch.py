@@ -42,7 +42,7 @@ class SceneRef:
 class BatchScenes:
     """Many structures' scenes in one device allocation, built in one pass."""
 
-    def __init__(self, structures, leaf_size=4, device=None):
+    def __init__(self, structures, leaf_size=8, device=None):
         lib = _lib.load()
         t = torch()
         self.device = require_cuda(device)
@@ -107,7 +107,7 @@ class BatchScenes:
 
 class BatchCCS:
     def __init__(self, structures, log2_rays, seeds, repeats=3, cap=64, precision='fp32', ehss=True, pa=False,
-                 leaf_size=4, launch=None, device=None, graph=True):
+                 leaf_size=8, launch=None, device=None, graph=True):
         S = len(structures)
         log2s = [int(log2_rays)] * S if np.isscalar(log2_rays) else [int(x) for x in log2_rays]
         seeds = [int(x) for x in (seeds if not np.isscalar(seeds) else [seeds] * S)]

@@ -24,7 +24,7 @@ import numpy as np
 from . import _lib
 from .device import empty, ptr, stream_handle, torch
 
-DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=6, chunk_rays=256, resolve_batch=24, smem_stack=16,
+DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=6, chunk_rays=256, resolve_batch=24, smem_stack=8,
                       count_tests=False)
 
 

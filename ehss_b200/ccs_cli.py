@@ -7,7 +7,7 @@ every replicate of a frame runs on the device in one fused launch (Sobol ->
 impact disk -> EHSS trace and/or BVH PA -> reduction), with the scene's LBVH
 built once and kept resident across replicates.  ``--threads`` is accepted
 and recorded (the GPU replaces worker threads); ``--leaf-size`` bounds the
-device LBVH leaves (1..8).
+device LBVH leaves (1..16).
 """
 from __future__ import annotations
 
@@ -149,7 +149,7 @@ def solve_frame(spheres, args, progress=True):
     pa = args.method in ("pa", "both")
     start = time.perf_counter()
     tick = time.perf_counter()
-    scene = Scene(spheres.centers, spheres.radii, leaf_size=min(int(args.leaf_size), 8))
+    scene = Scene(spheres.centers, spheres.radii, leaf_size=min(int(args.leaf_size), 16))
     setup_s = time.perf_counter() - tick
     seeds = seed_schedule(args.seed, args.repeats)
     rows = [dict(repeat=k + 1, seed=s) for k, s in enumerate(seeds)]
@@ -221,7 +221,7 @@ def parser():
     p.add_argument('--repeats', type=int, default=3, help='Independent scrambled Sobol replicates (default: 3)')
     p.add_argument('--seed', type=int, default=190003)
     p.add_argument('--threads', type=int, default=1, help='Accepted for compatibility; the GPU replaces CPU threads')
-    p.add_argument('--leaf-size', type=int, default=4, help='Maximum atoms per device LBVH leaf (1..8, default: 4)')
+    p.add_argument('--leaf-size', type=int, default=8, help='Maximum atoms per device LBVH leaf (1..16, default: 8)')
     p.add_argument('--max-collisions', type=int, default=64)
     p.add_argument('--probe-radius', type=float, default=1.4, help='Added probe radius in angstrom (default: 1.4, He scenario)')
     p.add_argument('--radii-json', type=Path, help='Overrides/additions to atomic VDW radii in angstrom, never effective radii')

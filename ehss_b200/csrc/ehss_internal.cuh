@@ -24,14 +24,15 @@ namespace ehss {
 // its children c = 0..3:
 //   f[0] = lo.x[c]  f[1] = hi.x[c]  f[2] = lo.y[c]  f[3] = hi.y[c]
 //   f[4] = lo.z[c]  f[5] = hi.z[c]  f[6] = child ref[c] (int bits)  f[7] = unused
-// child >= 0: node index; child < 0: leaf ~(first << 3 | (count - 1));
+// child >= 0: node index; child < 0: leaf ~(first << kLeafBits | (count - 1));
 // kEmptyChild marks an unused slot.  Node i is built from binary LBVH node i
 // with its grandchildren as children (children that are leaves, or subtrees
 // of at most leaf_size atoms, stay single slots), so only binary nodes at
 // even depth are ever referenced.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kSceneMagic = 0x45485353u;  // "EHSS"
-constexpr int kMaxLeaf = 8;
+constexpr int kLeafBits = 4;                 // leaf reference: atom count - 1 in the low bits
+constexpr int kMaxLeaf = 1 << kLeafBits;
 constexpr int kEmptyChild = INT32_MIN;
 constexpr int kStackDepth = 96;   // >= 3 x the deepest 4-wide tree (binary LBVH height <= 55)
 constexpr int kMaxWorkParts = 512;    // per-SM work ranges of the persistent kernel (workspace 4 KiB)

@@ -316,7 +316,7 @@ __global__ void k_emit_nodes(const BuildDesc* descs, int n_scenes, int64_t I_tot
                 u[0][k] = fminf(u[0][k], leaf_box[6 * (D.atom0 + a) + k]);
                 u[0][3 + k] = fmaxf(u[0][3 + k], leaf_box[6 * (D.atom0 + a) + 3 + k]);
             }
-        int ref = ~((0 << 3) | (int)(D.n - 1));
+        int ref = ~((0 << kLeafBits) | (int)(D.n - 1));
         write_node4(nodes, 0, u, &ref, 1, H->eps_box);
         H->depth = 1;
         H->n_nodes = 1;
@@ -337,13 +337,13 @@ __global__ void k_emit_nodes(const BuildDesc* descs, int n_scenes, int64_t I_tot
     auto classify = [&](int c, int& ref, const float*& box) -> bool {   // true: expandable internal node
         if (c < 0) {
             box = leaf_box + 6 * (D.atom0 + ~c);
-            ref = ~((~c) << 3);
+            ref = ~((~c) << kLeafBits);
             return false;
         }
         box = inner_box + 6 * (D.inner0 + c);
         int first = inner_range[2 * (D.inner0 + c)], last = inner_range[2 * (D.inner0 + c) + 1];
         int count = last - first + 1;
-        if (count <= D.leaf_size) { ref = ~((first << 3) | (count - 1)); return false; }
+        if (count <= D.leaf_size) { ref = ~((first << kLeafBits) | (count - 1)); return false; }
         ref = c;
         return true;
     };

@@ -177,7 +177,7 @@ __device__ __noinline__ int nearest(const SceneView& S, const double* o, const d
             }
         } else {
             int code = ~cur;
-            int first = code >> 3, cnt = (code & 7) + 1;
+            int first = code >> kLeafBits, cnt = (code & (kMaxLeaf - 1)) + 1;
             if (first + cnt > n_atoms) { ++st.errors; cnt = 0; }
             for (int k = first; k < first + cnt; ++k) {
                 if (k == last_rank) continue;
@@ -295,7 +295,7 @@ __device__ __noinline__ bool anyhit(const SceneView& S, const double* o, const d
             }
         } else {
             int code = ~cur;
-            int first = code >> 3, cnt = (code & 7) + 1;
+            int first = code >> kLeafBits, cnt = (code & (kMaxLeaf - 1)) + 1;
             if (first + cnt > n_atoms) { ++st.errors; cnt = 0; }
             for (int k = first; k < first + cnt; ++k) {
                 if (k == owner_rank) continue;
@@ -568,7 +568,7 @@ struct Walker {
     }
     __device__ __forceinline__ void leaf_tests(const SceneView& S, int ref, int last_rank, const LaneRay& L) {
         int code = ~ref;
-        int first = code >> 3, cnt = (code & 7) + 1;
+        int first = code >> kLeafBits, cnt = (code & (kMaxLeaf - 1)) + 1;
         if (first + cnt > S.h->n_atoms) { error = true; return; }
         for (int k = first; k < first + cnt; ++k) {
             if (k == last_rank) continue;

@@ -51,7 +51,7 @@ class Scene:
     (ehss_static.py:68-69).
     """
 
-    def __init__(self, centers, radii, leaf_size=4, device=None):
+    def __init__(self, centers, radii, leaf_size=8, device=None):
         lib = _lib.load()
         self.device = require_cuda(device)
         c = np.ascontiguousarray(centers, dtype=np.float64)
@@ -78,7 +78,7 @@ class Scene:
         self.radius = float(info.radius)
 
     @classmethod
-    def from_spheres(cls, spheres, leaf_size=4, device=None):
+    def from_spheres(cls, spheres, leaf_size=8, device=None):
         return cls(spheres.centers, spheres.radii, leaf_size, device)
 
     def source_rays(self, power, seed, first=0, n=None):
@@ -191,7 +191,7 @@ class PreparedStaticGPUEHSS:
         s = Spheres(spheres.centers, spheres.radii, deduplicate=False)
         if groups is not None:
             _check_groups(groups, len(s.radii))
-        scene = Scene.from_spheres(s, leaf_size=min(leaf_size, 8), device=device)
+        scene = Scene.from_spheres(s, leaf_size=min(leaf_size, 16), device=device)
         self.model = SimpleNamespace(spheres=s, scene=scene)
         self.scene = scene
         self.engine = GPUEHSSTransport(scene, precision=precision, threads=threads)
@@ -206,7 +206,7 @@ class SphereIndex:
         if kind not in ('bvh', 'octree') or leaf_size < 1:
             raise ValueError('Valid kind, positive leaf size and nonempty primitives required.')
         self.spheres = spheres
-        self.scene = Scene.from_spheres(spheres, leaf_size=min(int(leaf_size), 8), device=device)
+        self.scene = Scene.from_spheres(spheres, leaf_size=min(int(leaf_size), 16), device=device)
 
     def query(self, source):
         owners = getattr(source, 'owners', None)

@@ -171,7 +171,7 @@ class CCSServer:
 class DeviceExecutor:
     """The device side of the server: batched scene builds and fused block rounds."""
 
-    def __init__(self, leaf_size=4, cap=64, precision='fp32', launch=None, device=None):
+    def __init__(self, leaf_size=8, cap=64, precision='fp32', launch=None, device=None):
         from . import _lib
         from .device import require_cuda
         self.device = require_cuda(device)

@@ -70,7 +70,7 @@ int ehss_sobol_points(int dim, uint64_t seed, int64_t first, int64_t n, uint32_t
  * owned device buffer.  Replaces PreparedStaticCPUEHSS.__init__
  * (ehss_static.py:62-101) and SphereIndex.__init__ (pa_spatial.py:157-160):
  * the scene owns a copy of the coordinates (as the reference scene does,
- * ehss_static.py:68-69).  Results never depend on the tree.  leaf_size 1..8
+ * ehss_static.py:68-69).  Results never depend on the tree.  leaf_size 1..16
  * is the LBVH leaf bound (the reference's --leaf-size only shapes its own
  * tree and has no effect on results). */
 typedef struct ehss_scene_info {

@@ -50,7 +50,7 @@ def test_argument_validation_without_device(lib):
     sb, wb = ct.c_uint64(), ct.c_uint64()
     assert lib.ehss_scene_bytes(0, 4, ct.byref(sb), ct.byref(wb)) == _lib.ERR_VALUE
     assert b'atom count' in lib.ehss_last_error()
-    assert lib.ehss_scene_bytes(10, 9, ct.byref(sb), ct.byref(wb)) == _lib.ERR_VALUE
+    assert lib.ehss_scene_bytes(10, 17, ct.byref(sb), ct.byref(wb)) == _lib.ERR_VALUE
     assert lib.ehss_scene_bytes(1000, 4, ct.byref(sb), ct.byref(wb)) == 0
     assert sb.value % 256 == 0 and sb.value >= 256 + 999 * 64 + 1000 * (16 + 32 + 8)
     sv = (ct.c_uint32 * 300)(); sh = (ct.c_uint32 * 10)()
