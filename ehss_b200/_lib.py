@@ -21,6 +21,7 @@ STAT_BOX, STAT_SPHERE, STAT_QUERIES, STAT_GRAZING, STAT_FALLBACK, STAT_FP64, STA
 NSTATS = 8
 BLOCK_EHSS, BLOCK_PA = 1, 2
 LAUNCH_COUNT_TESTS = 1
+BUILD_EXTERIOR = 1
 FX_SCALE = 2.0 ** -40
 
 P = ct.c_void_p
@@ -30,7 +31,7 @@ I32, I64, U64 = ct.c_int32, ct.c_int64, ct.c_uint64
 class SceneInfo(ct.Structure):
     _fields_ = [('n_atoms', I64), ('n_nodes', I64), ('leaf_size', I32), ('depth', I32),
                 ('center', ct.c_double * 3), ('radius', ct.c_double), ('scale', ct.c_double),
-                ('rmax', ct.c_double), ('bytes', U64)]
+                ('rmax', ct.c_double), ('bytes', U64), ('n_active', I64), ('exterior', I32), ('reserved', I32)]
 
 
 class Block(ct.Structure):
@@ -59,6 +60,7 @@ _SIGNATURES = {
     'ehss_scene_build_noalloc': (ct.c_int, [I64, P, P, ct.c_int, P, U64, P]),
     'ehss_scenes_workspace_bytes': (ct.c_int, [ct.c_int, P, P]),
     'ehss_scenes_build': (ct.c_int, [ct.c_int, P, P, P, ct.c_int, P, P, P, U64, P]),
+    'ehss_scenes_build_ex': (ct.c_int, [ct.c_int, P, P, P, ct.c_int, P, P, P, U64, ct.c_uint32, P]),
     'ehss_scene_info_get': (ct.c_int, [P, P, P]),
     'ehss_source_rays': (ct.c_int, [P, ct.c_int, U64, I64, I64, P, P, P]),
     'ehss_trace': (ct.c_int, [P, I64, ct.c_int, ct.c_int, P, P, P, P, P, P, P, P, P]),

@@ -40,9 +40,14 @@ class SceneRef:
 
 
 class BatchScenes:
-    """Many structures' scenes in one device allocation, built in one pass."""
+    """Many structures' scenes in one device allocation, built in one pass.
 
-    def __init__(self, structures, leaf_size=8, device=None):
+    ``exterior=True`` builds exterior scenes (EHSS_BUILD_EXTERIOR): atoms
+    buried under their neighbours are left out of the trees, which the fused
+    block trace may use because all its rays start outside the union.
+    """
+
+    def __init__(self, structures, leaf_size=8, device=None, exterior=False):
         lib = _lib.load()
         t = torch()
         self.device = require_cuda(device)
@@ -89,6 +94,7 @@ class BatchScenes:
         self._scenes = (ct.c_void_p * S)(*self.scene_ptrs)
         self._sizes = (ct.c_uint64 * S)(*sizes)
         self.leaf_size = int(leaf_size)
+        self.flags = _lib.BUILD_EXTERIOR if exterior else 0
         self.scenes = [SceneRef(p, R, int(n), self.device) for p, R, n in zip(self.scene_ptrs, radii, self.n_atoms)]
         self.h2d_bytes = (N * 3 + N) * 8
 
@@ -100,18 +106,25 @@ class BatchScenes:
         if upload:
             self.upload()
         lib = _lib.load()
-        _lib.check(lib.ehss_scenes_build(len(self.scenes), self._xyz_ptrs, self._r_ptrs, self._n, self.leaf_size,
-                                         self._scenes, self._sizes, self.ws_ptr, self.ws_bytes,
-                                         stream_handle(self.device)), 'batched scene build')
+        _lib.check(lib.ehss_scenes_build_ex(len(self.scenes), self._xyz_ptrs, self._r_ptrs, self._n, self.leaf_size,
+                                            self._scenes, self._sizes, self.ws_ptr, self.ws_bytes, self.flags,
+                                            stream_handle(self.device)), 'batched scene build')
+
+    def info(self, i):
+        """Header of scene i (synchronises the stream)."""
+        info = _lib.SceneInfo()
+        _lib.check(_lib.load().ehss_scene_info_get(self.scene_ptrs[i], ct.byref(info), stream_handle(self.device)),
+                   'scene info')
+        return info
 
 
 class BatchCCS:
     def __init__(self, structures, log2_rays, seeds, repeats=3, cap=64, precision='fp32', ehss=True, pa=False,
-                 leaf_size=8, launch=None, device=None, graph=True):
+                 leaf_size=8, launch=None, device=None, graph=True, exterior=False):
         S = len(structures)
         log2s = [int(log2_rays)] * S if np.isscalar(log2_rays) else [int(x) for x in log2_rays]
         seeds = [int(x) for x in (seeds if not np.isscalar(seeds) else [seeds] * S)]
-        self.batch = BatchScenes(structures, leaf_size=leaf_size, device=device)
+        self.batch = BatchScenes(structures, leaf_size=leaf_size, device=device, exterior=exterior)
         self.device = self.batch.device
         self.scenes = self.batch.scenes
         self.n_atoms = self.batch.n_atoms

@@ -128,6 +128,21 @@ int ehss_scenes_build(int n_scenes, const double* const* xyz_dev, const double* 
                         workspace_dev, workspace_bytes, as_stream(stream));
 }
 
+int ehss_scenes_build_ex(int n_scenes, const double* const* xyz_dev, const double* const* radii_dev,
+                         const int64_t* n_atoms_host, int leaf_size, void* const* scenes_dev,
+                         const uint64_t* scene_bytes_host, void* workspace_dev, uint64_t workspace_bytes,
+                         uint32_t flags, void* stream) {
+    clear_error();
+    if (n_scenes < 1 || !xyz_dev || !radii_dev || !n_atoms_host || !scenes_dev || !scene_bytes_host ||
+        !workspace_dev) {
+        set_error("invalid arguments");
+        return EHSS_ERR_VALUE;
+    }
+    if (flags & ~EHSS_BUILD_EXTERIOR) { set_error("unknown build flags 0x%x", flags); return EHSS_ERR_VALUE; }
+    return build_scenes(n_scenes, xyz_dev, radii_dev, n_atoms_host, leaf_size, scenes_dev, scene_bytes_host,
+                        workspace_dev, workspace_bytes, as_stream(stream), (flags & EHSS_BUILD_EXTERIOR) != 0);
+}
+
 int ehss_scene_info_get(const void* scene_dev, ehss_scene_info* info, void* stream) {
     clear_error();
     if (!scene_dev || !info) { set_error("null pointer"); return EHSS_ERR_VALUE; }
@@ -148,6 +163,9 @@ int ehss_scene_info_get(const void* scene_dev, ehss_scene_info* info, void* stre
     info->scale = h.scale;
     info->rmax = h.rmax;
     info->bytes = h.bytes;
+    info->n_active = h.n_active;
+    info->exterior = h.exterior;
+    info->reserved = 0;
     return EHSS_OK;
 }
 

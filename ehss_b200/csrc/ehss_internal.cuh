@@ -52,6 +52,8 @@ struct alignas(256) SceneHeader {
     float scale_f;
     float rmax_f;
     float pad0;
+    int32_t n_active;      // atoms in the tree: all of them, or the exposed ones of an exterior scene
+    int32_t exterior;      // 1: buried atoms left out of the tree (valid for rays starting outside)
     uint64_t off_nodes, off_atoms, off_atoms64, off_ids, off_rank;
     uint64_t bytes;
 };
@@ -227,7 +229,7 @@ void sobol4_params(uint64_t seed, Sobol4Params* p);
 uint64_t build_workspace_bytes(int64_t N, int S);
 int build_scenes(int S, const double* const* xyz, const double* const* radii, const int64_t* n, int leaf_size,
                  void* const* scenes, const uint64_t* scene_bytes, void* workspace, uint64_t workspace_bytes,
-                 cudaStream_t stream);
+                 cudaStream_t stream, bool exterior = false);
 int launch_trace_rays(const void* scene, int64_t n, int cap, int precision, double* P, double* D,
                       const int64_t* last, int64_t* bounces, uint8_t* esc, uint8_t* unres, int32_t* hist,
                       uint64_t* stats, cudaStream_t stream);

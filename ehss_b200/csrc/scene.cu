@@ -39,7 +39,8 @@ struct BuildDesc {
     int64_t atom0;       // first global atom index
     int64_t inner0;      // first global internal-node index
     int32_t leaf_size;
-    int32_t pad;
+    int32_t exterior;
+    int64_t n_active;          // atoms in the tree (exterior scenes: the exposed atoms)
     double cmin[3], cext[3];   // centre box relative to the scene centre (filled by k_stats)
 };
 
@@ -58,6 +59,7 @@ struct BuildWork {
     float* leaf_box;         // [6*N]
     int32_t* inner_height;   // [I]
     uint32_t* arrivals;      // [I]
+    uint8_t* culled;         // [N] 1 = buried atom (exterior builds)
     void* cub_temp;
     size_t cub_bytes;
 };
@@ -153,7 +155,8 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
     return v;
 }
 
-__global__ void k_morton(const BuildDesc* descs, const int32_t* atom_scene, int64_t N, uint64_t* keys, int32_t* vals) {
+__global__ void k_morton(const BuildDesc* descs, const int32_t* atom_scene, int64_t N, const uint8_t* culled,
+                         uint64_t* keys, int32_t* vals) {
     int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (g >= N) return;
     int s = atom_scene[g];
@@ -169,7 +172,9 @@ __global__ void k_morton(const BuildDesc* descs, const int32_t* atom_scene, int6
         q[c] = (uint32_t)fmin(u * 1024.0, 1023.0);
     }
     uint32_t code = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
-    keys[g] = ((uint64_t)s << 30) | code;
+    // buried atoms of an exterior build sort after every exposed atom of their structure
+    uint64_t out = culled && D.exterior && culled[g] ? (1ull << 30) : 0ull;
+    keys[g] = ((uint64_t)s << 31) | out | code;
     vals[g] = (int32_t)i;
 }
 
@@ -193,9 +198,9 @@ __global__ void k_karras(const BuildDesc* descs, int n_scenes, int64_t I_total, 
         if (descs[mid].inner0 <= g) lo = mid; else hi = mid - 1;
     }
     const BuildDesc& D = descs[lo];
-    int n = (int)D.n;
+    int n = (int)D.n_active;
     int i = (int)(g - D.inner0);
-    if (i >= n - 1) return;   // structures with one atom own no internal node
+    if (i >= n - 1) return;   // structures with one (active) atom own no internal node
     int64_t base = D.atom0;
     int d = (delta(keys, base, n, i, i + 1) - delta(keys, base, n, i, i - 1)) >= 0 ? 1 : -1;
     int dmin = delta(keys, base, n, i, i - d);
@@ -245,11 +250,11 @@ __global__ void k_refit(const BuildDesc* descs, const int32_t* atom_scene, int64
     float b[6];
     atom_box(D, H, vals_sorted[g], b);
     for (int k = 0; k < 6; ++k) leaf_box[6 * g + k] = b[k];
-    if (D.n == 1) return;
+    if (D.n_active == 1 || g - D.atom0 >= D.n_active) return;    // no tree above, or a buried atom
     int node = parent_leaf[g];
     __threadfence();
     // a walk longer than any LBVH depth (Morton bits + duplicate bits) means a malformed link
-    for (int hops = 0; node >= 0 && node < D.n - 1 && hops < 128; ++hops) {
+    for (int hops = 0; node >= 0 && node < D.n_active - 1 && hops < 128; ++hops) {
         int64_t gi = D.inner0 + node;
         if (atomicAdd(&arrivals[gi], 1u) == 0) return;   // the sibling subtree is not finished yet
         __threadfence();
@@ -259,7 +264,7 @@ __global__ void k_refit(const BuildDesc* descs, const int32_t* atom_scene, int64
             int c = inner_child[2 * gi + side];
             const float* src;
             int hc;
-            if (c < 0 ? (~c >= D.n) : (c >= D.n - 1)) return;   // malformed link: leave the node unset
+            if (c < 0 ? (~c >= D.n_active) : (c >= D.n_active - 1)) return;   // malformed link: leave the node unset
             if (c < 0) { src = leaf_box + 6 * (D.atom0 + ~c); hc = 0; }
             else { src = inner_box + 6 * (D.inner0 + c); hc = __ldcg(inner_height + D.inner0 + c); }
             for (int k = 0; k < 3; ++k) {
@@ -303,20 +308,22 @@ __global__ void k_emit_nodes(const BuildDesc* descs, int n_scenes, int64_t I_tot
     if (g >= I_total) {
         const BuildDesc& D = descs[g - I_total];
         SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
-        if (D.n > D.leaf_size) {
+        H->n_active = (int32_t)D.n_active;
+        H->exterior = D.exterior;
+        if (D.n_active > D.leaf_size) {
             H->depth = inner_height[D.inner0];
-            H->n_nodes = (int32_t)(D.n - 1);
+            H->n_nodes = (int32_t)(D.n_active - 1);
             return;
         }
         // whole structure in one leaf below a single node
         float4* nodes = reinterpret_cast<float4*>(D.scene + H->off_nodes);
         float u[1][6] = {{CUDART_INF_F, CUDART_INF_F, CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F}};
-        for (int64_t a = 0; a < D.n; ++a)
+        for (int64_t a = 0; a < D.n_active; ++a)
             for (int k = 0; k < 3; ++k) {
                 u[0][k] = fminf(u[0][k], leaf_box[6 * (D.atom0 + a) + k]);
                 u[0][3 + k] = fmaxf(u[0][3 + k], leaf_box[6 * (D.atom0 + a) + 3 + k]);
             }
-        int ref = ~((0 << kLeafBits) | (int)(D.n - 1));
+        int ref = ~((0 << kLeafBits) | (int)(D.n_active - 1));
         write_node4(nodes, 0, u, &ref, 1, H->eps_box);
         H->depth = 1;
         H->n_nodes = 1;
@@ -329,7 +336,7 @@ __global__ void k_emit_nodes(const BuildDesc* descs, int n_scenes, int64_t I_tot
     }
     const BuildDesc& D = descs[lo];
     int i = (int)(g - D.inner0);
-    if (i >= D.n - 1 || D.n <= D.leaf_size) return;
+    if (i >= D.n_active - 1 || D.n_active <= D.leaf_size) return;
     SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
     float4* nodes = reinterpret_cast<float4*>(D.scene + H->off_nodes);
     // slot of a binary child: leaf reference when it is an atom or a subtree
@@ -400,6 +407,245 @@ __global__ void k_fill_scene_index(const BuildDesc* descs, int n_scenes, int32_t
 }
 
 // --------------------------------------------------------------------------
+// Exterior scenes: atoms that no ray starting outside the union can reach.
+//
+// A sphere B whose every surface point lies inside some other sphere at depth
+// >= m > 0 is never the nearest entry of a ray that starts outside the union
+// of the spheres or on its boundary (the impact disk and every bounce point
+// of the EHSS path): to reach B's surface the ray must cross the surface of
+// a covering sphere C at least m earlier, so C wins the (distance, id)
+// comparison strictly; and such a ray hits some other sphere whenever it hits
+// B, so any-hit results keep too.  Buried spheres are left out of the tree of
+// an exterior scene; outcomes are unchanged.
+//
+// Test (one warp per atom B, radius r): each neighbour C overlapping B gives
+// a cap on B's unit sphere, {s : |r s - (c_C - c_B)| <= r_C - h - mu}, i.e.
+// s.u_C >= cos(alpha_C) with u_C the unit direction to C.  B is buried when
+// every point of a latitude lattice -- rows at theta_k = (k + 1/2) pi / K,
+// ceil(2 K sin theta_k) + 1 points per row -- lies in some cap with h = r pi
+// / K: the lattice's geodesic covering radius is at most pi / K, so every
+// surface point is then within h of a covered sample and inside C at depth
+// >= mu.  Lattices K = 6, 12, 24 are tried in turn (a deeply buried atom is
+// proven on the coarse one); an atom is kept when a sample of the finest one
+// is uncovered.  mu = 1e-4 (r + d + r_C) + 2e-6 S bounds the FP32 error of
+// the cap test (at most 1e-5 (r + d + r_C) for the caps used, whose shrunk
+// radius is >= 0.05 (r + d + r_C)) and of the FP32 atom records ten times
+// over.  Dropping a neighbour can only keep an atom, so the fixed-size lists
+// below never make a wrong cut.
+// --------------------------------------------------------------------------
+constexpr int kLatticeLevels = 3;
+__host__ __device__ constexpr int lattice_k(int level) { return 6 << level; }   // K = 6, 12, 24
+constexpr int kLatticeRowsAll = 6 + 12 + 24;
+constexpr int kLatticeMax = 1120;      // > sum over the levels of sum_k (2 K sin theta_k + 2)
+constexpr int kExposureWarps = 8;
+constexpr int kMaxCaps = 96;
+constexpr int kFrontier = 64;
+constexpr int kLeafList = 64;
+
+struct ExposureWarp {
+    float4 cap[kMaxCaps];              // (u, cos alpha at the current lattice)
+    float2 dr[kMaxCaps];               // (distance, radius of C)
+    int front[2][kFrontier];
+    int leaves[kLeafList];
+    int n_front[2];
+    int n_leaves, n_caps, whole;
+};
+
+__device__ __forceinline__ float cap_cos(float r, float d, float rc_full, float h, float mS) {
+    const float L = r + d + rc_full;
+    const float rc = rc_full - h - 1e-4f * L - mS;     // shrunk radius of C
+    if (rc < 0.05f * L || d >= r + rc) return 3.f;    // too thin to count, or no cap
+    return (r * r + d * d - rc * rc) / (2.f * r * d);
+}
+
+__global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* descs, const int32_t* atom_scene,
+                                                                  int64_t N, uint8_t* culled) {
+    __shared__ float4 dirs[kLatticeMax];
+    __shared__ int row_start[kLatticeRowsAll + 1];
+    __shared__ int level_start[kLatticeLevels + 1];
+    __shared__ ExposureWarp wsm[kExposureWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        int t = 0, row = 0;
+        for (int lv = 0; lv < kLatticeLevels; ++lv) {
+            level_start[lv] = t;
+            const int K = lattice_k(lv);
+            for (int k = 0; k < K; ++k, ++row) {
+                row_start[row] = t;
+                t += (int)ceilf(2.0f * K * sinf((k + 0.5f) * 3.14159265358979f / K)) + 1;
+            }
+        }
+        t = t < kLatticeMax ? t : kLatticeMax;
+        row_start[kLatticeRowsAll] = t;
+        level_start[kLatticeLevels] = t;
+    }
+    __syncthreads();
+    const int n_dirs = row_start[kLatticeRowsAll];
+    for (int t = threadIdx.x; t < n_dirs; t += blockDim.x) {
+        int row = 0;
+        while (row + 1 < kLatticeRowsAll && row_start[row + 1] <= t) ++row;
+        const int K = row < 6 ? 6 : (row < 18 ? 12 : 24);
+        const int k = row - (row < 6 ? 0 : (row < 18 ? 6 : 18));
+        const int L = row_start[row + 1] - row_start[row];
+        float st, ct, sp, cp;
+        sincosf((k + 0.5f) * 3.14159265358979f / K, &st, &ct);
+        sincosf(6.28318530717959f * (float)(t - row_start[row]) / (float)L, &sp, &cp);
+        dirs[t] = make_float4(st * cp, st * sp, ct, 0.f);
+    }
+    __syncthreads();
+    ExposureWarp& W = wsm[warp];
+    for (int64_t g = blockIdx.x * (int64_t)kExposureWarps + warp; g < N; g += (int64_t)gridDim.x * kExposureWarps) {
+        BuildDesc& D = descs[atom_scene[g]];
+        const SceneView S = scene_view(D.scene);
+        const int j = (int)(g - D.atom0);          // leaf-order position: neighbouring warps share subtrees
+        const float4 b = S.atoms[j];
+        const float mS = 2e-6f * S.h->scale_f;
+        const float h_fine = b.w * 3.14159265358979f / lattice_k(kLatticeLevels - 1);
+        if (lane == 0) {
+            W.front[0][0] = 0;
+            W.n_front[0] = 1;
+            W.n_leaves = W.n_caps = W.whole = 0;
+        }
+        __syncwarp();
+        // 1. leaves whose boxes meet B's box (breadth first, one node per lane)
+        const float lo[3] = {b.x - b.w, b.y - b.w, b.z - b.w}, hi[3] = {b.x + b.w, b.y + b.w, b.z + b.w};
+        const int n_nodes = S.h->n_nodes;
+        int cur = 0;
+        for (int level = 0; level < 64; ++level) {
+            const int nf = min(W.n_front[cur], kFrontier);
+            __syncwarp();
+            if (nf == 0) break;
+            if (lane == 0) W.n_front[cur ^ 1] = 0;
+            __syncwarp();
+            for (int k = lane; k < nf; k += 32) {
+                const int node = W.front[cur][k];
+                if (node < 0 || node >= n_nodes) continue;       // malformed: drop (keeps atoms)
+                const float4* nd = S.nodes + 8 * (int64_t)node;
+                const float4 lx = nd[0], hx = nd[1], ly = nd[2], hy = nd[3], lz = nd[4], hz = nd[5], rf = nd[6];
+                const float cl[3][4] = {{lx.x, lx.y, lx.z, lx.w}, {ly.x, ly.y, ly.z, ly.w}, {lz.x, lz.y, lz.z, lz.w}};
+                const float ch[3][4] = {{hx.x, hx.y, hx.z, hx.w}, {hy.x, hy.y, hy.z, hy.w}, {hz.x, hz.y, hz.z, hz.w}};
+                const int refs[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z),
+                                     __float_as_int(rf.w)};
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    if (refs[c] == kEmptyChild) continue;
+                    bool hit = true;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) hit = hit && cl[a][c] <= hi[a] && ch[a][c] >= lo[a];
+                    if (!hit) continue;
+                    if (refs[c] >= 0) {
+                        int slot = atomicAdd(&W.n_front[cur ^ 1], 1);
+                        if (slot < kFrontier) W.front[cur ^ 1][slot] = refs[c];
+                    } else {
+                        int slot = atomicAdd(&W.n_leaves, 1);
+                        if (slot < kLeafList) W.leaves[slot] = refs[c];
+                    }
+                }
+            }
+            __syncwarp();
+            cur ^= 1;
+        }
+        // 2. neighbours with a cap on the finest lattice, two leaves per pass (16 lanes each)
+        const int nl = min(W.n_leaves, kLeafList);
+        for (int l = lane >> 4; l < ((nl + 1) & ~1); l += 2) {
+            if (l >= nl) continue;
+            const int code = ~W.leaves[l];
+            const int first = code >> kLeafBits, cnt = (code & (kMaxLeaf - 1)) + 1;
+            const int k = first + (lane & 15);
+            if ((lane & 15) >= cnt || k >= S.h->n_atoms || k == j) continue;
+            const float4 a = S.atoms[k];
+            const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+            const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+            if (d + b.w <= a.w - 1e-4f * (b.w + d + a.w) - mS) { W.whole = 1; continue; }   // C alone holds B
+            const float key = cap_cos(b.w, d, a.w, h_fine, mS);
+            if (!(key < 1.f)) continue;
+            if (key <= -1.f) { W.whole = 1; continue; }
+            const int slot = atomicAdd(&W.n_caps, 1);
+            if (slot < kMaxCaps) {
+                W.cap[slot] = make_float4(dx / d, dy / d, dz / d, key);
+                W.dr[slot] = make_float2(d, a.w);
+            }
+        }
+        __syncwarp();
+        const int nc = min(W.n_caps, kMaxCaps);
+        bool buried = W.whole != 0;
+        // largest caps first (rank sort on cos alpha, ties by slot)
+        if (!buried && nc > 1) {
+            float4 mc[3];
+            float2 md[3];
+            int rk[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const int i = lane + 32 * q;
+                rk[q] = -1;
+                if (i < nc) {
+                    mc[q] = W.cap[i];
+                    md[q] = W.dr[i];
+                    int r = 0;
+                    for (int o = 0; o < nc; ++o) {
+                        const float w = W.cap[o].w;
+                        r += (w < mc[q].w || (w == mc[q].w && o < i)) ? 1 : 0;
+                    }
+                    rk[q] = r;
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                if (rk[q] >= 0) { W.cap[rk[q]] = mc[q]; W.dr[rk[q]] = md[q]; }
+            __syncwarp();
+        }
+        // 3. lattices from coarse to fine: every sample inside some cap?
+        bool exposed = nc == 0 && !buried;
+        for (int lv = 0; lv < kLatticeLevels && !buried && !exposed; ++lv) {
+            const float h = b.w * 3.14159265358979f / lattice_k(lv);
+            bool whole = false;
+            for (int i = lane; i < nc; i += 32) {
+                const float2 dr = W.dr[i];
+                const float c = cap_cos(b.w, dr.x, dr.y, h, mS);
+                W.cap[i].w = c;
+                whole = whole || c <= -1.f;
+            }
+            __syncwarp();
+            if (__any_sync(0xffffffffu, whole)) { buried = true; break; }
+            const int s0 = level_start[lv], ns = level_start[lv + 1] - s0;
+            const int stride = ns % 97 ? 97 : 89;      // scattered visiting order, coprime to ns
+            bool uncovered = false;
+            for (int base = 0; base < ns && !uncovered; base += 32) {
+                bool miss = false;
+                const int t = base + lane;
+                if (t < ns) {
+                    const float4 s = dirs[s0 + (int)(((int64_t)t * stride) % ns)];
+                    bool covered = false;
+                    for (int c = 0; c < nc && !covered; ++c) {
+                        const float4 u = W.cap[c];
+                        covered = s.x * u.x + s.y * u.y + s.z * u.z >= u.w;
+                    }
+                    miss = !covered;
+                }
+                uncovered = __any_sync(0xffffffffu, miss);
+            }
+            if (!uncovered) buried = true;
+            else if (lv == kLatticeLevels - 1) exposed = true;
+            __syncwarp();
+        }
+        if (lane == 0) {
+            culled[D.atom0 + S.ids[j]] = buried ? 1 : 0;
+            if (buried) atomicAdd(reinterpret_cast<unsigned long long*>(&D.n_active), ~0ull);   // -1
+        }
+        __syncwarp();
+    }
+}
+
+// A structure whose atoms all tested buried (impossible for a bounded union:
+// its boundary lies on some exposed sphere) falls back to the full tree.
+__global__ void k_finish_exposure(BuildDesc* descs, int n_scenes) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_scenes) return;
+    if (descs[s].n_active < 1) { descs[s].n_active = descs[s].n; descs[s].exterior = 0; }
+}
+
+// --------------------------------------------------------------------------
 // Host side
 // --------------------------------------------------------------------------
 static size_t cub_sort_bytes(int64_t N) {
@@ -425,13 +671,14 @@ uint64_t build_workspace_bytes(int64_t N, int S) {
     b += align256(24ull * N);           // leaf_box
     b += align256(4ull * I);            // inner_height
     b += align256(4ull * I);            // arrivals
+    b += align256(1ull * N);            // culled
     b += align256(cub_sort_bytes(N));
     return b + 256;
 }
 
 int build_scenes(int S, const double* const* xyz, const double* const* radii, const int64_t* n, int leaf_size,
                  void* const* scenes, const uint64_t* scene_bytes, void* workspace, uint64_t workspace_bytes,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, bool exterior) {
     if (S < 1) { set_error("at least one structure required"); return EHSS_ERR_VALUE; }
     if (leaf_size < 1 || leaf_size > kMaxLeaf) { set_error("leaf_size must be 1..%d", kMaxLeaf); return EHSS_ERR_VALUE; }
     int64_t N = 0, I = 0;
@@ -457,7 +704,8 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
         }
         BuildDesc& D = host[s];
         D.xyz = xyz[s]; D.radii = radii[s]; D.scene = (char*)scenes[s];
-        D.n = n[s]; D.atom0 = N; D.inner0 = I; D.leaf_size = leaf_size; D.pad = 0;
+        D.n = n[s]; D.atom0 = N; D.inner0 = I; D.leaf_size = leaf_size; D.exterior = exterior ? 1 : 0;
+        D.n_active = n[s];
         N += n[s];
         I += n[s] - 1;
     }
@@ -485,6 +733,7 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
     W.leaf_box = (float*)p; p += align256(24ull * N);
     W.inner_height = (int32_t*)p; p += align256(4ull * Ia);
     W.arrivals = (uint32_t*)p; p += align256(4ull * Ia);
+    W.culled = (uint8_t*)p; p += align256(1ull * N);
     W.cub_temp = p;
     W.cub_bytes = cub_sort_bytes(N);
 
@@ -510,29 +759,49 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
     auto blocks = [&](int64_t count) { return (unsigned)((count + T - 1) / T); };
     k_fill_scene_index<<<S, 256, 0, stream>>>(W.descs, S, W.atom_scene);
     k_stats<<<S, 256, 0, stream>>>(W.descs, S);
-    k_morton<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, W.keys_in, W.vals_in);
-    int end_bit = 30;
-    while ((1ll << (end_bit - 30)) < S) ++end_bit;
-    size_t cub_bytes = W.cub_bytes;
-    rc = cuda_status(cub::DeviceRadixSort::SortPairs(W.cub_temp, cub_bytes, W.keys_in, W.keys_out, W.vals_in,
-                                                     W.vals_out, (int)N, 0, end_bit, stream), "LBVH key sort");
-    if (rc) return rc;
-    // parent links start at -1 so that a missing link ends a refit walk
-    rc = cuda_status(cudaMemsetAsync(W.parent_leaf, 0xff, 4ull * N, stream), "LBVH parent reset");
-    if (rc) return rc;
-    if (I > 0) {
-        rc = cuda_status(cudaMemsetAsync(W.arrivals, 0, 4ull * I, stream), "LBVH arrival reset");
-        if (!rc) rc = cuda_status(cudaMemsetAsync(W.parent_inner, 0xff, 4ull * I, stream), "LBVH parent reset");
-        if (rc) return rc;
-        k_karras<<<blocks(I), T, 0, stream>>>(W.descs, S, I, W.keys_out, W.inner_child, W.inner_range,
-                                              W.parent_inner, W.parent_leaf);
+    int end_bit = 31;
+    while ((1ll << (end_bit - 31)) < S) ++end_bit;
+    // one pass: Morton keys -> sort -> Karras hierarchy -> refit -> node and atom records
+    auto tree_pass = [&](const uint8_t* culled) -> int {
+        k_morton<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, culled, W.keys_in, W.vals_in);
+        size_t cub_bytes = W.cub_bytes;
+        int r = cuda_status(cub::DeviceRadixSort::SortPairs(W.cub_temp, cub_bytes, W.keys_in, W.keys_out, W.vals_in,
+                                                            W.vals_out, (int)N, 0, end_bit, stream), "LBVH key sort");
+        if (r) return r;
+        // parent links start at -1 so that a missing link ends a refit walk
+        r = cuda_status(cudaMemsetAsync(W.parent_leaf, 0xff, 4ull * N, stream), "LBVH parent reset");
+        if (r) return r;
+        if (I > 0) {
+            r = cuda_status(cudaMemsetAsync(W.arrivals, 0, 4ull * I, stream), "LBVH arrival reset");
+            if (!r) r = cuda_status(cudaMemsetAsync(W.parent_inner, 0xff, 4ull * I, stream), "LBVH parent reset");
+            if (r) return r;
+            k_karras<<<blocks(I), T, 0, stream>>>(W.descs, S, I, W.keys_out, W.inner_child, W.inner_range,
+                                                  W.parent_inner, W.parent_leaf);
+        }
+        k_refit<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, W.vals_out, W.inner_child, W.parent_inner,
+                                             W.parent_leaf, W.inner_box, W.leaf_box, W.inner_height, W.arrivals);
+        k_emit_nodes<<<blocks(I + S), T, 0, stream>>>(W.descs, S, I, W.inner_child, W.inner_range, W.inner_box,
+                                                      W.leaf_box, W.inner_height);
+        k_emit_atoms<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, W.vals_out);
+        return cuda_status(cudaGetLastError(), "LBVH build launch");
+    };
+    rc = tree_pass(nullptr);
+    if (rc || !exterior) return rc;
+    // exterior scenes: mark buried atoms with the full tree, then rebuild over the exposed ones
+    {
+        int64_t want = (N + kExposureWarps - 1) / kExposureWarps;
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exposure, 32 * kExposureWarps, 0) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        int64_t cap = (int64_t)per_sm * sm_count();
+        unsigned grid = (unsigned)(want < cap ? want : cap);
+        k_exposure<<<grid, 32 * kExposureWarps, 0, stream>>>(W.descs, W.atom_scene, N, W.culled);
     }
-    k_refit<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, W.vals_out, W.inner_child, W.parent_inner,
-                                         W.parent_leaf, W.inner_box, W.leaf_box, W.inner_height, W.arrivals);
-    k_emit_nodes<<<blocks(I + S), T, 0, stream>>>(W.descs, S, I, W.inner_child, W.inner_range, W.inner_box,
-                                                  W.leaf_box, W.inner_height);
-    k_emit_atoms<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, W.vals_out);
-    return cuda_status(cudaGetLastError(), "LBVH build launch");
+    k_finish_exposure<<<(S + 127) / 128, 128, 0, stream>>>(W.descs, S);
+    rc = cuda_status(cudaGetLastError(), "exposure launch");
+    if (rc) return rc;
+    return tree_pass(W.culled);
 }
 
 }  // namespace ehss

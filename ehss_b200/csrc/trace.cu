@@ -380,7 +380,8 @@ __global__ void __launch_bounds__(128) k_trace_rays(const void* scene, int64_t n
     LocalStats st;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t first = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    bool ok = S.h->magic == kSceneMagic && S.h->status == 0;
+    // exterior scenes hold only the atoms reachable from outside the union: not for arbitrary rays
+    bool ok = S.h->magic == kSceneMagic && S.h->status == 0 && S.h->exterior == 0;
     for (int64_t i = first; i < n; i += stride) {
         double o[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
         double d[3] = {D[3 * i], D[3 * i + 1], D[3 * i + 2]};
@@ -410,7 +411,8 @@ __global__ void __launch_bounds__(128) k_pa_rays(const void* scene, int64_t n, c
     SceneView S = scene_view(scene);
     LocalStats st;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    bool ok = S.h->magic == kSceneMagic && S.h->status == 0;
+    // exterior scenes hold only the atoms reachable from outside the union: not for arbitrary rays
+    bool ok = S.h->magic == kSceneMagic && S.h->status == 0 && S.h->exterior == 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
         double o[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
         double d[3] = {D[3 * i], D[3 * i + 1], D[3 * i + 2]};

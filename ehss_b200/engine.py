@@ -51,7 +51,7 @@ class Scene:
     (ehss_static.py:68-69).
     """
 
-    def __init__(self, centers, radii, leaf_size=8, device=None):
+    def __init__(self, centers, radii, leaf_size=8, device=None, exterior=False):
         lib = _lib.load()
         self.device = require_cuda(device)
         c = np.ascontiguousarray(centers, dtype=np.float64)
@@ -68,12 +68,21 @@ class Scene:
         xyz_d = to_device(c, np.float64, self.device)
         r_d = to_device(r, np.float64, self.device)
         ws, ws_addr = _aligned_buffer(wb.value, self.device)
-        _lib.check(lib.ehss_scene_build(self.n_atoms, xyz_d.data_ptr(), r_d.data_ptr(), self.leaf_size, self.ptr,
-                                        sb.value, ws_addr, wb.value, stream), 'scene build')
+        if exterior:
+            # buried atoms left out of the tree: valid for the fused block trace only
+            _lib.check(lib.ehss_scenes_build_ex(1, (ct.c_void_p * 1)(xyz_d.data_ptr()),
+                                                (ct.c_void_p * 1)(r_d.data_ptr()), (ct.c_int64 * 1)(self.n_atoms),
+                                                self.leaf_size, (ct.c_void_p * 1)(self.ptr), (ct.c_uint64 * 1)(sb.value),
+                                                ws_addr, wb.value, _lib.BUILD_EXTERIOR, stream), 'scene build')
+        else:
+            _lib.check(lib.ehss_scene_build(self.n_atoms, xyz_d.data_ptr(), r_d.data_ptr(), self.leaf_size, self.ptr,
+                                            sb.value, ws_addr, wb.value, stream), 'scene build')
         info = _lib.SceneInfo()
         _lib.check(lib.ehss_scene_info_get(self.ptr, ct.byref(info), stream), 'scene build')   # synchronises
         del ws, xyz_d, r_d
         self.info = info
+        self.exterior = bool(info.exterior)
+        self.n_active = int(info.n_active)
         self.center = np.array(info.center[:])
         self.radius = float(info.radius)
 
@@ -123,6 +132,8 @@ class GPUEHSSTransport:
     """EHSS tracer on one prepared scene (CPUEHSSTransport.trace contract)."""
 
     def __init__(self, scene, precision='fp32', threads=1):
+        if getattr(scene, 'exterior', False):
+            raise ValueError('an exterior scene holds only atoms reachable from outside; trace needs a full scene')
         self.scene = scene
         self.precision = _precision(precision)
         self.threads = threads

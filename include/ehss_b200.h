@@ -83,6 +83,9 @@ typedef struct ehss_scene_info {
     double scale;             /* max |c_j - center| + r_j */
     double rmax;              /* largest radius */
     uint64_t bytes;           /* bytes used in the scene buffer */
+    int64_t n_active;         /* atoms in the tree: n_atoms, or the exposed atoms of an exterior scene */
+    int32_t exterior;         /* 1: built with EHSS_BUILD_EXTERIOR */
+    int32_t reserved;
 } ehss_scene_info;
 
 /* Bytes of the scene buffer and of the build workspace for n_atoms. */
@@ -119,6 +122,22 @@ int ehss_scenes_build(int n_scenes, const double* const* xyz_dev, const double* 
                       const int64_t* n_atoms_host, int leaf_size, void* const* scenes_dev,
                       const uint64_t* scene_bytes_host, void* workspace_dev, uint64_t workspace_bytes,
                       void* stream);
+
+/* Batched build with options.  No counterpart in the reference.
+ * EHSS_BUILD_EXTERIOR leaves buried atoms out of the tree: an atom whose
+ * whole surface lies inside other atoms (tested on latitude lattices whose
+ * covering radius is added to the required depth) is never the nearest entry
+ * of a ray that starts outside the union of the spheres, which every
+ * impact-disk ray and every EHSS bounce point does, so the fused block trace
+ * (ehss_trace_blocks) gives the same outcomes on an exterior scene with fewer
+ * tests.  ehss_trace and ehss_pa_anyhit take arbitrary rays and report every
+ * ray of an exterior scene as an error (EHSS_STAT_ERRORS).  flags = 0 is
+ * ehss_scenes_build. */
+#define EHSS_BUILD_EXTERIOR 1u
+int ehss_scenes_build_ex(int n_scenes, const double* const* xyz_dev, const double* const* radii_dev,
+                         const int64_t* n_atoms_host, int leaf_size, void* const* scenes_dev,
+                         const uint64_t* scene_bytes_host, void* workspace_dev, uint64_t workspace_bytes,
+                         uint32_t flags, void* stream);
 
 /* Copy the scene header to the host (synchronises `stream`).  Fails with
  * EHSS_ERR_VALUE when the build found a non-positive or non-finite radius or

@@ -68,3 +68,55 @@ def test_autotuner_returns_a_valid_faster_or_equal_launch(eb):
     ref = BlockPlan(jobs)
     ref.run()
     assert [r['ehss_angstrom2'] for r in plan.collect()] == [r['ehss_angstrom2'] for r in ref.collect()]
+
+
+def _lattice(k=6, spacing=1.2, radius=1.5):
+    g = np.stack(np.meshgrid(*[np.arange(k)] * 3, indexing='ij'), -1).reshape(-1, 3) * spacing
+    return g.astype(np.float64), np.full(len(g), radius)
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_exterior_scenes_give_identical_blocks(eb, precision):
+    """Buried atoms left out of the trees change no outcome of any block."""
+    from ehss_b200.batch import BatchCCS
+    from ehss_b200.blocks import DEFAULT_LAUNCH
+    structures = _structures([1, 3, 40, 700, 3000], seed=31) + [_lattice()]
+    seeds = [5, 6, 7, 8, 9, 10]
+    kw = dict(repeats=2, cap=64, precision=precision, pa=True, graph=False,
+              launch=dict(DEFAULT_LAUNCH, count_tests=True))
+    full = BatchCCS(structures, 13, seeds, **kw)
+    ext = BatchCCS(structures, 13, seeds, exterior=True, **kw)
+    a, b = full.run(), ext.run()
+    keys = ('ehss_angstrom2', 'pa_angstrom2', 'pa_from_same_rays_angstrom2', 'unresolved_rays', 'escaped_rays',
+            'collision_histogram', 'collision_contribution_angstrom2')
+    for x, y in zip(a, b):
+        for rx, ry in zip(x['runs'], y['runs']):
+            assert {k: rx[k] for k in keys} == {k: ry[k] for k in keys}
+    infos = [ext.batch.info(i) for i in range(len(structures))]
+    assert all(i.exterior == 1 and 1 <= i.n_active <= i.n_atoms for i in infos)
+    assert infos[-1].n_active == 216 - 64            # the lattice's 4^3 inner atoms are buried
+    assert infos[4].n_active < infos[4].n_atoms      # and so are a globule's core atoms
+    assert all(full.batch.info(i).n_active == n for i, n in enumerate(full.n_atoms))
+    tests = lambda out: sum(r['sphere_tests'] for o in out for r in o['runs'])
+    assert tests(b) < tests(a)
+
+
+def test_exterior_scene_refused_for_explicit_rays(eb):
+    import torch
+    from ehss_b200 import _lib
+    c, r = _lattice()
+    sc = eb.Scene(c, r, exterior=True)
+    assert sc.exterior and sc.n_active == 216 - 64
+    with pytest.raises(ValueError):
+        eb.GPUEHSSTransport(sc)
+    n = 4
+    o = torch.zeros((n, 3), dtype=torch.float64, device='cuda')
+    o[:, 0] = -50.0
+    d = torch.zeros((n, 3), dtype=torch.float64, device='cuda')
+    d[:, 0] = 1.0
+    own = torch.full((n,), -1, dtype=torch.int64, device='cuda')
+    blocked = torch.zeros(n, dtype=torch.uint8, device='cuda')
+    stats = torch.zeros(_lib.NSTATS, dtype=torch.int64, device='cuda')
+    _lib.check(_lib.load().ehss_pa_anyhit(sc.ptr, n, o.data_ptr(), d.data_ptr(), own.data_ptr(), blocked.data_ptr(),
+                                          stats.data_ptr(), torch.cuda.current_stream().cuda_stream))
+    assert int(stats[_lib.STAT_ERRORS]) == n and int(blocked.sum()) == 0

@@ -56,6 +56,12 @@ def test_argument_validation_without_device(lib):
     sv = (ct.c_uint32 * 300)(); sh = (ct.c_uint32 * 10)()
     assert lib.ehss_sobol_scramble(9, 0, sv, sh) == _lib.ERR_VALUE
     assert lib.ehss_trace(None, 1, 0, 1, *([None] * 8), None) == _lib.ERR_VALUE
+    one = (ct.c_void_p * 1)(1024)
+    assert lib.ehss_scenes_build_ex(1, one, one, (ct.c_int64 * 1)(10), 8, one, (ct.c_uint64 * 1)(1 << 20), 1024,
+                                    1 << 20, 2, None) == _lib.ERR_VALUE
+    assert b'unknown build flags' in lib.ehss_last_error()
+    assert lib.ehss_scenes_build_ex(0, one, one, (ct.c_int64 * 1)(10), 8, one, (ct.c_uint64 * 1)(1 << 20), 1024,
+                                    1 << 20, 1, None) == _lib.ERR_VALUE
     with pytest.raises(ValueError):
         _lib.check(_lib.ERR_VALUE)
 
@@ -87,6 +93,7 @@ def test_struct_layouts_match_header():
     assert ct.sizeof(_lib.Block) == 544 and _lib.Block.basis.offset == 0 and _lib.Block.base.offset == 480
     assert ct.sizeof(_lib.BlockResult) == 8 * (5 + _lib.NSTATS)
     assert ct.sizeof(_lib.Launch) == 32
+    assert ct.sizeof(_lib.SceneInfo) == 96 and _lib.SceneInfo.n_active.offset == 80
 
 
 def test_workload_generators():
