@@ -2,7 +2,8 @@
 
 ``BatchCCS`` is the public entry for the batched form: it takes host arrays
 of many structures of uneven size, stages them in pinned memory, builds every
-LBVH in one pass of the builder kernels (ehss_scenes_build), runs all
+LBVH in one pass of the builder kernels (ehss_scenes_build_ex; exterior
+scenes by default, since every block ray starts outside the union), runs all
 (structure, replicate) blocks in one persistent launch (optionally replayed
 from a CUDA graph) and returns per-structure EHSS/PA summaries with the
 reference CLI's replicate statistics (ccs_cli.summarize, ccs_cli.py:163-167).
@@ -120,7 +121,7 @@ class BatchScenes:
 
 class BatchCCS:
     def __init__(self, structures, log2_rays, seeds, repeats=3, cap=64, precision='fp32', ehss=True, pa=False,
-                 leaf_size=8, launch=None, device=None, graph=True, exterior=False):
+                 leaf_size=8, launch=None, device=None, graph=True, exterior=True):
         S = len(structures)
         log2s = [int(log2_rays)] * S if np.isscalar(log2_rays) else [int(x) for x in log2_rays]
         seeds = [int(x) for x in (seeds if not np.isscalar(seeds) else [seeds] * S)]

@@ -149,7 +149,8 @@ def solve_frame(spheres, args, progress=True):
     pa = args.method in ("pa", "both")
     start = time.perf_counter()
     tick = time.perf_counter()
-    scene = Scene(spheres.centers, spheres.radii, leaf_size=min(int(args.leaf_size), 16))
+    # block rays all start on the impact disk, so buried atoms can leave the tree (exterior scene)
+    scene = Scene(spheres.centers, spheres.radii, leaf_size=min(int(args.leaf_size), 16), exterior=True)
     setup_s = time.perf_counter() - tick
     seeds = seed_schedule(args.seed, args.repeats)
     rows = [dict(repeat=k + 1, seed=s) for k, s in enumerate(seeds)]

@@ -187,7 +187,8 @@ class DeviceExecutor:
 
     def build(self, structures):
         from .batch import BatchScenes
-        scenes = BatchScenes(structures, leaf_size=self.leaf_size, device=self.device)
+        # every block ray starts on the impact disk: exterior scenes give the same outcomes
+        scenes = BatchScenes(structures, leaf_size=self.leaf_size, device=self.device, exterior=True)
         scenes.build()
         return [(scenes, i) for i in range(len(structures))]
 

@@ -84,7 +84,7 @@ def test_exterior_scenes_give_identical_blocks(eb, precision):
     seeds = [5, 6, 7, 8, 9, 10]
     kw = dict(repeats=2, cap=64, precision=precision, pa=True, graph=False,
               launch=dict(DEFAULT_LAUNCH, count_tests=True))
-    full = BatchCCS(structures, 13, seeds, **kw)
+    full = BatchCCS(structures, 13, seeds, exterior=False, **kw)
     ext = BatchCCS(structures, 13, seeds, exterior=True, **kw)
     a, b = full.run(), ext.run()
     keys = ('ehss_angstrom2', 'pa_angstrom2', 'pa_from_same_rays_angstrom2', 'unresolved_rays', 'escaped_rays',
