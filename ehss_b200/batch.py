@@ -139,7 +139,7 @@ class BatchCCS:
         self.rays = self.plan.rays
         self.use_graph = graph
         self.h2d_bytes = self.batch.h2d_bytes
-        self.d2h_bytes = self.plan.results.numel() + 16 * self.plan.hist.numel()
+        self.d2h_bytes = self.plan.d2h_bytes
 
     # -- stages ---------------------------------------------------------------
     def upload(self):
@@ -155,17 +155,24 @@ class BatchCCS:
 
     def download(self):
         blocks = self.plan.collect()
-        out = [dict(structure=s, atoms=sc.n_atoms, runs=[]) for s, sc in enumerate(self.scenes)]
-        for b in blocks:
-            out[b['tag'][0]]['runs'].append(b)
-        for o in out:
-            runs = o['runs']
-            if 'ehss_angstrom2' in runs[0]:
-                o['ehss_angstrom2'] = summarize([r['ehss_angstrom2'] for r in runs])
-                o['ehss_tail_bound_mean_angstrom2'] = float(np.mean([r['tail_bound_angstrom2'] for r in runs]))
-                o['ehss_unresolved_rays_total'] = int(sum(r['unresolved_rays'] for r in runs))
-            if 'pa_angstrom2' in runs[0]:
-                o['pa_angstrom2'] = summarize([r['pa_angstrom2'] for r in runs])
+        S, R = len(self.scenes), self.repeats
+        out = [dict(structure=s, atoms=sc.n_atoms, runs=blocks[s * R:(s + 1) * R]) for s, sc in enumerate(self.scenes)]
+
+        def summaries(key):
+            a = np.array([b[key] for b in blocks]).reshape(S, R)
+            mean = a.mean(axis=1).tolist()
+            sd = a.std(axis=1, ddof=1).tolist() if R > 1 else [None] * S
+            return [dict(mean=m, sd=d, sem=d / math.sqrt(R) if d is not None else None, replicates=R)
+                    for m, d in zip(mean, sd)]
+        if 'ehss_angstrom2' in blocks[0]:
+            ehss = summaries('ehss_angstrom2')
+            tails = np.array([b['tail_bound_angstrom2'] for b in blocks]).reshape(S, R).mean(axis=1).tolist()
+            unres = np.array([b['unresolved_rays'] for b in blocks]).reshape(S, R).sum(axis=1).tolist()
+            for o, e, t, u in zip(out, ehss, tails, unres):
+                o.update(ehss_angstrom2=e, ehss_tail_bound_mean_angstrom2=t, ehss_unresolved_rays_total=int(u))
+        if 'pa_angstrom2' in blocks[0]:
+            for o, p in zip(out, summaries('pa_angstrom2')):
+                o['pa_angstrom2'] = p
         return out
 
     def run(self):

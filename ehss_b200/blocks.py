@@ -24,6 +24,8 @@ import numpy as np
 from . import _lib
 from .device import empty, ptr, stream_handle, torch
 
+_RESULT_WORDS = ct.sizeof(_lib.BlockResult) // 8
+_STATS0 = _lib.BlockResult.stats.offset // 8
 DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=6, chunk_rays=256, resolve_batch=24, smem_stack=8,
                       count_tests=False)
 
@@ -78,9 +80,19 @@ class BlockPlan:
         self.hist_entries = offset
         raw = np.frombuffer(bytes(host), dtype=np.uint8)
         self.blocks_dev = t.from_numpy(raw.copy()).to(self.device)
-        self.results = t.zeros(n * ct.sizeof(_lib.BlockResult), dtype=t.uint8, device=self.device)
-        self.hist = t.zeros(max(offset, 1), dtype=t.int64, device=self.device)
-        self.ledger = t.zeros(max(offset, 1), dtype=t.int64, device=self.device)
+        # block totals, histograms and ledgers in one buffer: one copy back to the host
+        H = max(offset, 1)
+        nw = n * _RESULT_WORDS
+        self.packed = t.zeros(nw + 2 * H, dtype=t.int64, device=self.device)
+        self.results, self.hist, self.ledger = self.packed[:nw], self.packed[nw:nw + H], self.packed[nw + H:]
+        self.hist_len = H
+        self.d2h_bytes = self.packed.numel() * 8
+        self._radius = [float(j.scene.radius) for j in self.jobs]
+        self._w = np.array([np.pi * R * R / (1 << j.log2_rays) for R, j in zip(self._radius, self.jobs)])
+        self._offsets = [int(host[i].hist_offset) for i in range(n)]
+        self._w_entry = np.zeros(H)
+        for i, j in enumerate(self.jobs):
+            self._w_entry[self._offsets[i]:self._offsets[i] + j.cap + 1] = self._w[i]
         wb = ct.c_uint64()
         _lib.check(lib.ehss_blocks_workspace_bytes(n, ct.byref(wb)), 'blocks')
         self.work = t.zeros(int(wb.value) // 8 + 1, dtype=t.int64, device=self.device)
@@ -116,35 +128,45 @@ class BlockPlan:
             self.enqueue()
 
     def collect(self):
-        """Copy results to the host; returns one dict per block (synchronises)."""
-        raw = self.results.cpu().numpy().tobytes()
-        res = (_lib.BlockResult * len(self.jobs)).from_buffer_copy(raw)
-        hist = self.hist.cpu().numpy().astype(np.int64)
-        ledger = self.ledger.cpu().numpy().astype(np.uint64)
+        """Copy results to the host; returns one dict per block (synchronises).
+
+        One device-to-host copy brings the block totals, histograms and
+        ledgers; the read-out is vectorised over blocks.
+        """
+        packed = self.packed.cpu().numpy().view(np.uint64)
+        n = len(self.jobs)
+        nw = n * _RESULT_WORDS
+        res = packed[:nw].reshape(n, _RESULT_WORDS)
+        stats = res[:, _STATS0:_STATS0 + _lib.NSTATS]
+        errors = stats[:, _lib.STAT_ERRORS]
+        if errors.any():
+            i = int(np.flatnonzero(errors)[0])
+            raise _lib.EHSSDeviceError(f'block {self.jobs[i].tag!r}: {int(errors[i])} bounded device failures')
+        H = self.hist_len
+        hist = packed[nw:nw + H].astype(np.int64).tolist()
+        ledger = (packed[nw + H:nw + 2 * H].astype(np.float64) * _lib.FX_SCALE * self._w_entry).tolist()
+        w = self._w
+        ehss = (w * (res[:, 0].astype(np.float64) * _lib.FX_SCALE)).tolist()
+        hits, unres, esc, pab = (res[:, k].tolist() for k in (1, 2, 3, 4))
+        cols = {k: stats[:, k].tolist() for k in (_lib.STAT_SPHERE, _lib.STAT_BOX, _lib.STAT_GRAZING,
+                                                  _lib.STAT_FALLBACK, _lib.STAT_QUERIES)}
+        wl = w.tolist()
         out = []
-        offset = 0
-        for j, r in zip(self.jobs, res):
-            n = 1 << j.log2_rays
-            R = j.scene.radius
-            w = np.pi * R * R / n
-            stats = np.array(r.stats[:], dtype=np.uint64)
-            if stats[_lib.STAT_ERRORS]:
-                raise _lib.EHSSDeviceError(f'block {j.tag!r}: {int(stats[_lib.STAT_ERRORS])} bounded device failures')
-            h = hist[offset:offset + j.cap + 1]
-            lg = ledger[offset:offset + j.cap + 1].astype(np.float64) * _lib.FX_SCALE * w
-            offset += j.cap + 1
-            angle = r.angle_fx * _lib.FX_SCALE
-            d = dict(tag=j.tag, rays=n, weight=w, radius=R, stats=stats)
+        for i, j in enumerate(self.jobs):
+            wi = wl[i]
+            d = dict(tag=j.tag, rays=1 << j.log2_rays, weight=wi, radius=self._radius[i], stats=stats[i])
             if j.ehss:
-                d.update(ehss_angstrom2=w * angle, pa_from_same_rays_angstrom2=w * r.hits,
-                         tail_bound_angstrom2=2 * w * r.unresolved, unresolved_rays=int(r.unresolved),
-                         escaped_rays=int(r.escaped), collision_histogram=h.tolist(),
-                         collision_contribution_angstrom2=lg.tolist(),
-                         sphere_tests=int(stats[_lib.STAT_SPHERE]), box_tests=int(stats[_lib.STAT_BOX]),
-                         grazing_queries=int(stats[_lib.STAT_GRAZING]),
-                         fp64_fallback_queries=int(stats[_lib.STAT_FALLBACK]), queries=int(stats[_lib.STAT_QUERIES]))
+                o, e = self._offsets[i], self._offsets[i] + j.cap + 1
+                d.update(ehss_angstrom2=ehss[i], pa_from_same_rays_angstrom2=wi * hits[i],
+                         tail_bound_angstrom2=2 * wi * unres[i], unresolved_rays=int(unres[i]),
+                         escaped_rays=int(esc[i]), collision_histogram=hist[o:e],
+                         collision_contribution_angstrom2=ledger[o:e],
+                         sphere_tests=int(cols[_lib.STAT_SPHERE][i]), box_tests=int(cols[_lib.STAT_BOX][i]),
+                         grazing_queries=int(cols[_lib.STAT_GRAZING][i]),
+                         fp64_fallback_queries=int(cols[_lib.STAT_FALLBACK][i]),
+                         queries=int(cols[_lib.STAT_QUERIES][i]))
             if j.pa:
-                d.update(pa_angstrom2=w * r.pa_blocked, pa_blocked_rays=int(r.pa_blocked))
+                d.update(pa_angstrom2=wi * pab[i], pa_blocked_rays=int(pab[i]))
             out.append(d)
         return out
 

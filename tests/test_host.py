@@ -160,3 +160,43 @@ def test_coherent_enumeration_is_the_sobol_point_set(lib, m, seed):
         digits = (m - 5) // 4
         top = pts.reshape(-1, 32, 4) >> np.uint32(30 - digits)
         assert (top == top[:, :1, :]).all(axis=(1, 2)).mean() == 1.0
+
+
+def test_block_readout_matches_per_block_formulas():
+    """BlockPlan.collect's vectorised read-out against the per-block definitions
+    omega = w angle_fx 2^-40, pa = w hits, tail = 2 w unresolved (host only)."""
+    import torch
+    from ehss_b200 import _lib
+    from ehss_b200.blocks import BlockJob, BlockPlan, _RESULT_WORDS, _STATS0
+
+    class FakeScene:
+        ptr, radius, device, n_atoms = 0x10000, 12.5, torch.device('cpu'), 10
+
+    spec = [(10, 1, 4, True), (12, 2, 8, False), (14, 3, 2, True)]
+    jobs = [BlockJob(FakeScene(), lg, seed, cap=cap, pa=pa, tag=i) for i, (lg, seed, cap, pa) in enumerate(spec)]
+    plan = BlockPlan(jobs, device=torch.device('cpu'))
+    rng = np.random.default_rng(3)
+    words = plan.packed.numpy().view(np.uint64)
+    n = len(jobs)
+    res = rng.integers(0, 2 ** 50, size=(n, _RESULT_WORDS), dtype=np.uint64)
+    res[:, _STATS0 + _lib.STAT_ERRORS] = 0
+    words[:n * _RESULT_WORDS] = res.ravel()
+    words[n * _RESULT_WORDS:] = rng.integers(0, 2 ** 40, size=len(words) - n * _RESULT_WORDS, dtype=np.uint64)
+    out = plan.collect()
+    hist = words[n * _RESULT_WORDS:n * _RESULT_WORDS + plan.hist_len]
+    ledger = words[n * _RESULT_WORDS + plan.hist_len:]
+    off = 0
+    for j, r, d in zip(jobs, res, out):
+        w = np.pi * 12.5 * 12.5 / (1 << j.log2_rays)
+        assert d['ehss_angstrom2'] == w * (int(r[0]) * _lib.FX_SCALE)
+        assert d['pa_from_same_rays_angstrom2'] == w * int(r[1])
+        assert d['tail_bound_angstrom2'] == 2 * w * int(r[2])
+        assert d['collision_histogram'] == hist[off:off + j.cap + 1].astype(np.int64).tolist()
+        assert d['collision_contribution_angstrom2'] == (ledger[off:off + j.cap + 1].astype(np.float64)
+                                                          * _lib.FX_SCALE * w).tolist()
+        assert ('pa_angstrom2' in d) == j.pa and (not j.pa or d['pa_angstrom2'] == w * int(r[4]))
+        off += j.cap + 1
+    res[1, _STATS0 + _lib.STAT_ERRORS] = 2
+    words[:n * _RESULT_WORDS] = res.ravel()
+    with pytest.raises(_lib.EHSSDeviceError):
+        plan.collect()
