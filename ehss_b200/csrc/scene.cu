@@ -418,35 +418,47 @@ __global__ void k_fill_scene_index(const BuildDesc* descs, int n_scenes, int32_t
 // B, so any-hit results keep too.  Buried spheres are left out of the tree of
 // an exterior scene; outcomes are unchanged.
 //
-// Test (one warp per atom B, radius r): each neighbour C overlapping B gives
+// Test (one warp per atom B, radius r).  Each neighbour C overlapping B gives
 // a cap on B's unit sphere, {s : |r s - (c_C - c_B)| <= r_C - h - mu}, i.e.
-// s.u_C >= cos(alpha_C) with u_C the unit direction to C.  B is buried when
-// every point of a latitude lattice -- rows at theta_k = (k + 1/2) pi / K,
-// ceil(2 K sin theta_k) + 1 points per row -- lies in some cap with h = r pi
-// / K: the lattice's geodesic covering radius is at most pi / K, so every
-// surface point is then within h of a covered sample and inside C at depth
-// >= mu.  Lattices K = 6, 12, 24 are tried in turn (a deeply buried atom is
-// proven on the coarse one); an atom is kept when a sample of the finest one
-// is uncovered.  mu = 1e-4 (r + d + r_C) + 2e-6 S bounds the FP32 error of
-// the cap test (at most 1e-5 (r + d + r_C) for the caps used, whose shrunk
-// radius is >= 0.05 (r + d + r_C)) and of the FP32 atom records ten times
-// over.  Dropping a neighbour can only keep an atom, so the fixed-size lists
-// below never make a wrong cut.
+// s.u_C >= cos(alpha_C) with u_C the unit direction to C.  Lattice K is the
+// latitude lattice with rows theta_k = (k + 1/2) pi / K and ceil(2 K sin
+// theta_k) + 1 points per row; its geodesic covering radius is at most pi / K.
+// A sample of lattice K is "covered" when it lies in some cap with h = r pi /
+// K: every surface point within geodesic pi / K of it is then inside C at
+// depth >= mu.  B is buried when every surface point is certified that way:
+//   level 0: every sample of lattice 12 is tested; the uncovered ones U are
+//            kept.  A point is certified unless it lies within pi / 12 of
+//            some U.
+//   level i: lattice K = 12 * 2^i is tested only within geodesic 3 pi / K of
+//            each U of the previous level (every point within pi / (K / 2) of
+//            U has its nearest lattice-K sample there); the uncovered ones
+//            become the next U.  No U left: buried.
+// Levels stop at K = 48; more than kMaxOpen open samples, or any left at the
+// last level, keep the atom (deeper levels and more open samples cut more
+// atoms but cost more build time than they save in the trace of one batch).  mu = 1e-4 (r + d + r_C) + 2e-6 S bounds the
+// FP32 error of the cap test (at most 1e-5 (r + d + r_C) for the caps used,
+// whose shrunk radius is >= 0.05 (r + d + r_C)) and of the FP32 atom records
+// ten times over; the candidate search is widened by 5 % and one sample per
+// row so that rounding cannot drop a sample.  Dropping a neighbour, or
+// declaring an atom exposed, only keeps atoms, so the fixed-size lists below
+// never make a wrong cut.
 // --------------------------------------------------------------------------
-constexpr int kLatticeLevels = 3;
-__host__ __device__ constexpr int lattice_k(int level) { return 6 << level; }   // K = 6, 12, 24
-constexpr int kLatticeRowsAll = 6 + 12 + 24;
-constexpr int kLatticeMax = 1120;      // > sum over the levels of sum_k (2 K sin theta_k + 2)
+constexpr int kLattice0 = 12;          // the fully tested lattice
+constexpr int kRefineLevels = 2;       // then K = 24, 48 around open samples
+constexpr int kLattice0Max = 256;      // > sum_k (2 K sin theta_k + 2) for K = 12
 constexpr int kExposureWarps = 8;
 constexpr int kMaxCaps = 96;
 constexpr int kFrontier = 64;
 constexpr int kLeafList = 64;
+constexpr int kMaxOpen = 8;
+constexpr float kPi = 3.14159265358979f;
 
 struct ExposureWarp {
     float4 cap[kMaxCaps];              // (u, cos alpha at the current lattice)
     float2 dr[kMaxCaps];               // (distance, radius of C)
     int front[2][kFrontier];
     int leaves[kLeafList];
+    int open[2][kMaxOpen];             // open samples (row << 16 | index) of the last two levels
     int n_front[2];
     int n_leaves, n_caps, whole;
 };
@@ -458,41 +470,60 @@ __device__ __forceinline__ float cap_cos(float r, float d, float rc_full, float 
     return (r * r + d * d - rc * rc) / (2.f * r * d);
 }
 
+__device__ __forceinline__ int lattice_row_len(int K, float theta) {
+    return (int)ceilf(2.0f * K * sinf(theta)) + 1;
+}
+
+// Caps for lattice spacing h; true when one cap alone holds the whole sphere.
+__device__ __forceinline__ bool set_caps(ExposureWarp& W, int nc, float r, float h, float mS, int lane) {
+    bool whole = false;
+    for (int i = lane; i < nc; i += 32) {
+        const float2 dr = W.dr[i];
+        const float c = cap_cos(r, dr.x, dr.y, h, mS);
+        W.cap[i].w = c;
+        whole = whole || c <= -1.f;
+    }
+    __syncwarp();
+    return __any_sync(0xffffffffu, whole);
+}
+
+__device__ __forceinline__ bool in_some_cap(const ExposureWarp& W, int nc, float sx, float sy, float sz) {
+    for (int c = 0; c < nc; ++c) {
+        const float4 u = W.cap[c];
+        if (sx * u.x + sy * u.y + sz * u.z >= u.w) return true;
+    }
+    return false;
+}
+
 __global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* descs, const int32_t* atom_scene,
                                                                   int64_t N, uint8_t* culled) {
-    __shared__ float4 dirs[kLatticeMax];
-    __shared__ int row_start[kLatticeRowsAll + 1];
-    __shared__ int level_start[kLatticeLevels + 1];
+    __shared__ float4 dirs0[kLattice0Max];      // lattice 12: (x, y, z, id bits)
+    __shared__ int row_start0[kLattice0 + 1];
     __shared__ ExposureWarp wsm[kExposureWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu, below = (1u << lane) - 1u;
     if (threadIdx.x == 0) {
-        int t = 0, row = 0;
-        for (int lv = 0; lv < kLatticeLevels; ++lv) {
-            level_start[lv] = t;
-            const int K = lattice_k(lv);
-            for (int k = 0; k < K; ++k, ++row) {
-                row_start[row] = t;
-                t += (int)ceilf(2.0f * K * sinf((k + 0.5f) * 3.14159265358979f / K)) + 1;
-            }
+        int t = 0;
+        for (int k = 0; k < kLattice0; ++k) {
+            row_start0[k] = t;
+            t += lattice_row_len(kLattice0, (k + 0.5f) * kPi / kLattice0);
         }
-        t = t < kLatticeMax ? t : kLatticeMax;
-        row_start[kLatticeRowsAll] = t;
-        level_start[kLatticeLevels] = t;
+        row_start0[kLattice0] = t < kLattice0Max ? t : kLattice0Max;
     }
     __syncthreads();
-    const int n_dirs = row_start[kLatticeRowsAll];
-    for (int t = threadIdx.x; t < n_dirs; t += blockDim.x) {
-        int row = 0;
-        while (row + 1 < kLatticeRowsAll && row_start[row + 1] <= t) ++row;
-        const int K = row < 6 ? 6 : (row < 18 ? 12 : 24);
-        const int k = row - (row < 6 ? 0 : (row < 18 ? 6 : 18));
-        const int L = row_start[row + 1] - row_start[row];
+    const int n0 = row_start0[kLattice0];
+    for (int t = threadIdx.x; t < n0; t += blockDim.x) {
+        int k = 0;
+        while (k + 1 < kLattice0 && row_start0[k + 1] <= t) ++k;
+        const int l = t - row_start0[k];
+        const int L = row_start0[k + 1] - row_start0[k];
         float st, ct, sp, cp;
-        sincosf((k + 0.5f) * 3.14159265358979f / K, &st, &ct);
-        sincosf(6.28318530717959f * (float)(t - row_start[row]) / (float)L, &sp, &cp);
-        dirs[t] = make_float4(st * cp, st * sp, ct, 0.f);
+        sincosf((k + 0.5f) * kPi / kLattice0, &st, &ct);
+        sincosf(2.f * kPi * (float)l / (float)L, &sp, &cp);
+        dirs0[t] = make_float4(st * cp, st * sp, ct, __int_as_float((k << 16) | l));
     }
     __syncthreads();
+    const int stride0 = n0 % 97 ? 97 : 89;          // scattered visiting order, coprime to n0
     ExposureWarp& W = wsm[warp];
     for (int64_t g = blockIdx.x * (int64_t)kExposureWarps + warp; g < N; g += (int64_t)gridDim.x * kExposureWarps) {
         BuildDesc& D = descs[atom_scene[g]];
@@ -500,7 +531,7 @@ __global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* des
         const int j = (int)(g - D.atom0);          // leaf-order position: neighbouring warps share subtrees
         const float4 b = S.atoms[j];
         const float mS = 2e-6f * S.h->scale_f;
-        const float h_fine = b.w * 3.14159265358979f / lattice_k(kLatticeLevels - 1);
+        const float h_fine = b.w * kPi / (kLattice0 << kRefineLevels);
         if (lane == 0) {
             W.front[0][0] = 0;
             W.n_front[0] = 1;
@@ -545,14 +576,17 @@ __global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* des
             __syncwarp();
             cur ^= 1;
         }
-        // 2. neighbours with a cap on the finest lattice, two leaves per pass (16 lanes each)
+        // 2. neighbours with a cap on the finest lattice; lanes split over leaves of <= 8 or <= 16 atoms
         const int nl = min(W.n_leaves, kLeafList);
-        for (int l = lane >> 4; l < ((nl + 1) & ~1); l += 2) {
+        const int per_leaf = S.h->leaf_size <= 8 ? 8 : 16, leaves_per_pass = 32 / per_leaf;
+        const int slot_in_leaf = lane % per_leaf;
+        for (int base = 0; base < nl; base += leaves_per_pass) {
+            const int l = base + lane / per_leaf;
             if (l >= nl) continue;
             const int code = ~W.leaves[l];
             const int first = code >> kLeafBits, cnt = (code & (kMaxLeaf - 1)) + 1;
-            const int k = first + (lane & 15);
-            if ((lane & 15) >= cnt || k >= S.h->n_atoms || k == j) continue;
+            const int k = first + slot_in_leaf;
+            if (slot_in_leaf >= cnt || k >= S.h->n_atoms || k == j) continue;
             const float4 a = S.atoms[k];
             const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
             const float d = sqrtf(dx * dx + dy * dy + dz * dz);
@@ -595,39 +629,115 @@ __global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* des
                 if (rk[q] >= 0) { W.cap[rk[q]] = mc[q]; W.dr[rk[q]] = md[q]; }
             __syncwarp();
         }
-        // 3. lattices from coarse to fine: every sample inside some cap?
         bool exposed = nc == 0 && !buried;
-        for (int lv = 0; lv < kLatticeLevels && !buried && !exposed; ++lv) {
-            const float h = b.w * 3.14159265358979f / lattice_k(lv);
-            bool whole = false;
-            for (int i = lane; i < nc; i += 32) {
-                const float2 dr = W.dr[i];
-                const float c = cap_cos(b.w, dr.x, dr.y, h, mS);
-                W.cap[i].w = c;
-                whole = whole || c <= -1.f;
-            }
-            __syncwarp();
-            if (__any_sync(0xffffffffu, whole)) { buried = true; break; }
-            const int s0 = level_start[lv], ns = level_start[lv + 1] - s0;
-            const int stride = ns % 97 ? 97 : 89;      // scattered visiting order, coprime to ns
-            bool uncovered = false;
-            for (int base = 0; base < ns && !uncovered; base += 32) {
-                bool miss = false;
+        // 3a. lattice 12, every sample; open samples recorded
+        int n_open = 0;
+        if (!buried && !exposed) {
+            buried = set_caps(W, nc, b.w, b.w * kPi / kLattice0, mS, lane);
+            for (int base = 0; base < n0 && !buried && !exposed; base += 32) {
                 const int t = base + lane;
-                if (t < ns) {
-                    const float4 s = dirs[s0 + (int)(((int64_t)t * stride) % ns)];
-                    bool covered = false;
-                    for (int c = 0; c < nc && !covered; ++c) {
-                        const float4 u = W.cap[c];
-                        covered = s.x * u.x + s.y * u.y + s.z * u.z >= u.w;
-                    }
-                    miss = !covered;
+                bool miss = false;
+                int id = 0;
+                if (t < n0) {
+                    const float4 s = dirs0[(int)(((int64_t)t * stride0) % n0)];
+                    miss = !in_some_cap(W, nc, s.x, s.y, s.z);
+                    id = __float_as_int(s.w);
                 }
-                uncovered = __any_sync(0xffffffffu, miss);
+                const unsigned m = __ballot_sync(full, miss);
+                const int at = n_open + __popc(m & below);
+                if (miss && at < kMaxOpen) W.open[0][at] = id;
+                n_open += __popc(m);
+                exposed = n_open > kMaxOpen;
             }
-            if (!uncovered) buried = true;
-            else if (lv == kLatticeLevels - 1) exposed = true;
             __syncwarp();
+            if (!buried && !exposed && n_open == 0) buried = true;
+        }
+        // 3b. finer lattices around the open samples
+        int side = 0;
+        for (int lv = 1; lv <= kRefineLevels && !buried && !exposed; ++lv) {
+            const int K = kLattice0 << lv, Kp = K >> 1;
+            const float alpha = 1.05f * 3.f * kPi / K;            // 3 pi / K, widened
+            const float ca = cosf(alpha);
+            if (set_caps(W, nc, b.w, b.w * kPi / K, mS, lane)) { buried = true; break; }
+            int n_next = 0;
+            for (int u = 0; u < n_open && !exposed; ++u) {
+                const int idU = W.open[side][u];
+                const int kU = idU >> 16, lU = idU & 0xffff;
+                const float thU = (kU + 0.5f) * kPi / Kp;
+                const float phU = 2.f * kPi * (float)lU / (float)lattice_row_len(Kp, thU);
+                float sU, cU;
+                sincosf(thU, &sU, &cU);
+                const int kmin = max(0, (int)ceilf((thU - alpha) * K / kPi - 0.5f) - 1);
+                const int kmax = min(K - 1, (int)floorf((thU + alpha) * K / kPi - 0.5f) + 1);
+                const int nrows = kmax - kmin + 1;                 // <= 9
+                // row q on lane q: samples l0 .. l0 + cnt - 1 (mod L) lie within alpha of U
+                int rk = 0, rL = 1, rl0 = 0, rcnt = 0;
+                float rs = 0.f, rc = 1.f;
+                if (lane < nrows) {
+                    rk = kmin + lane;
+                    const float th = (rk + 0.5f) * kPi / K;
+                    sincosf(th, &rs, &rc);
+                    rL = lattice_row_len(K, th);
+                    const float den = sU * rs;
+                    const float rhs = den > 1e-6f ? (ca - cU * rc) / den : -2.f;
+                    if (rhs <= -1.f) { rl0 = 0; rcnt = rL; }
+                    else if (rhs <= 1.f) {
+                        const float dphi = acosf(rhs) + 2.f * kPi / rL;
+                        const int a0 = (int)ceilf((phU - dphi) * rL / (2.f * kPi));
+                        const int a1 = (int)floorf((phU + dphi) * rL / (2.f * kPi));
+                        rcnt = a1 - a0 + 1;
+                        if (rcnt >= rL) { rl0 = 0; rcnt = rL; }
+                        else { rl0 = a0; rcnt = max(rcnt, 0); }
+                    }
+                }
+                int incl = rcnt;                                   // inclusive scan over the rows
+#pragma unroll
+                for (int o = 1; o < 16; o <<= 1) {
+                    const int v = __shfl_up_sync(full, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int total = __shfl_sync(full, incl, nrows - 1);
+                for (int base = 0; base < total && !exposed; base += 32) {
+                    const int t = base + lane;
+                    bool miss = false;
+                    int id = 0;
+                    // row of candidate t: first q with incl[q] > t
+                    int q_sel = -1, excl = 0;
+                    for (int q = 0; q < nrows; ++q) {
+                        const int iq = __shfl_sync(full, incl, q);
+                        const int cq = __shfl_sync(full, rcnt, q);
+                        if (q_sel < 0 && t < iq) { q_sel = q; excl = iq - cq; }
+                    }
+                    const int qk = __shfl_sync(full, rk, q_sel < 0 ? 0 : q_sel);
+                    const int qL = __shfl_sync(full, rL, q_sel < 0 ? 0 : q_sel);
+                    const int ql0 = __shfl_sync(full, rl0, q_sel < 0 ? 0 : q_sel);
+                    const float qs = __shfl_sync(full, rs, q_sel < 0 ? 0 : q_sel);
+                    const float qc = __shfl_sync(full, rc, q_sel < 0 ? 0 : q_sel);
+                    if (t < total && q_sel >= 0) {
+                        int l = (ql0 + (t - excl)) % qL;
+                        if (l < 0) l += qL;
+                        float sp, cp;
+                        sincosf(2.f * kPi * (float)l / (float)qL, &sp, &cp);
+                        miss = !in_some_cap(W, nc, qs * cp, qs * sp, qc);
+                        id = (qk << 16) | l;
+                        if (miss)
+                            for (int o = 0; o < n_next && o < kMaxOpen; ++o)
+                                if (W.open[side ^ 1][o] == id) { miss = false; break; }   // already open
+                    }
+                    const unsigned m = __ballot_sync(full, miss);
+                    const int at = n_next + __popc(m & below);
+                    __syncwarp();
+                    if (miss && at < kMaxOpen) W.open[side ^ 1][at] = id;
+                    n_next += __popc(m);
+                    exposed = n_next > kMaxOpen;
+                    __syncwarp();
+                }
+            }
+            if (exposed) break;
+            if (n_next == 0) buried = true;
+            else if (lv == kRefineLevels) exposed = true;
+            n_open = n_next;
+            side ^= 1;
         }
         if (lane == 0) {
             culled[D.atom0 + S.ids[j]] = buried ? 1 : 0;
