@@ -151,22 +151,25 @@ class BlockPlan:
         cols = {k: stats[:, k].tolist() for k in (_lib.STAT_SPHERE, _lib.STAT_BOX, _lib.STAT_GRAZING,
                                                   _lib.STAT_FALLBACK, _lib.STAT_QUERIES)}
         wl = w.tolist()
+        pa_same = (w * res[:, 1].astype(np.float64)).tolist()
+        tail = (2 * w * res[:, 2].astype(np.float64)).tolist()
+        pa_area = (w * res[:, 4].astype(np.float64)).tolist()
+        sph, box, graz, fall, qry = (cols[k] for k in (_lib.STAT_SPHERE, _lib.STAT_BOX, _lib.STAT_GRAZING,
+                                                      _lib.STAT_FALLBACK, _lib.STAT_QUERIES))
         out = []
         for i, j in enumerate(self.jobs):
-            wi = wl[i]
-            d = dict(tag=j.tag, rays=1 << j.log2_rays, weight=wi, radius=self._radius[i], stats=stats[i])
+            d = {'tag': j.tag, 'rays': 1 << j.log2_rays, 'weight': wl[i], 'radius': self._radius[i], 'stats': stats[i]}
             if j.ehss:
-                o, e = self._offsets[i], self._offsets[i] + j.cap + 1
-                d.update(ehss_angstrom2=ehss[i], pa_from_same_rays_angstrom2=wi * hits[i],
-                         tail_bound_angstrom2=2 * wi * unres[i], unresolved_rays=int(unres[i]),
-                         escaped_rays=int(esc[i]), collision_histogram=hist[o:e],
-                         collision_contribution_angstrom2=ledger[o:e],
-                         sphere_tests=int(cols[_lib.STAT_SPHERE][i]), box_tests=int(cols[_lib.STAT_BOX][i]),
-                         grazing_queries=int(cols[_lib.STAT_GRAZING][i]),
-                         fp64_fallback_queries=int(cols[_lib.STAT_FALLBACK][i]),
-                         queries=int(cols[_lib.STAT_QUERIES][i]))
+                o = self._offsets[i]
+                e = o + j.cap + 1
+                d.update({'ehss_angstrom2': ehss[i], 'pa_from_same_rays_angstrom2': pa_same[i],
+                          'tail_bound_angstrom2': tail[i], 'unresolved_rays': unres[i], 'escaped_rays': esc[i],
+                          'collision_histogram': hist[o:e], 'collision_contribution_angstrom2': ledger[o:e],
+                          'sphere_tests': sph[i], 'box_tests': box[i], 'grazing_queries': graz[i],
+                          'fp64_fallback_queries': fall[i], 'queries': qry[i]})
             if j.pa:
-                d.update(pa_angstrom2=wi * pab[i], pa_blocked_rays=int(pab[i]))
+                d['pa_angstrom2'] = pa_area[i]
+                d['pa_blocked_rays'] = pab[i]
             out.append(d)
         return out
 
