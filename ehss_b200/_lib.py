@@ -45,6 +45,15 @@ class BlockResult(ct.Structure):
                 ('stats', U64 * NSTATS)]
 
 
+class Residual(ct.Structure):
+    _fields_ = [('o', ct.c_double * 3), ('d', ct.c_double * 3), ('din', ct.c_double * 3), ('block', I32),
+                ('last_rank', I32), ('bounces', I32), ('reserved', I32)]
+
+
+class Extension(ct.Structure):
+    _fields_ = [('angle_fx', U64), ('escaped', U64), ('unresolved', U64), ('continued', U64)]
+
+
 class Launch(ct.Structure):
     _fields_ = [('block_threads', I32), ('ctas_per_sm', I32), ('chunk_rays', I32), ('resolve_batch', I32),
                 ('precisions', I32), ('options', I32), ('smem_stack', I32), ('reserved', I32)]
@@ -70,6 +79,8 @@ _SIGNATURES = {
     'ehss_blocks_prepare': (ct.c_int, [P, ct.c_int, P, ct.c_int, P]),
     'ehss_blocks_workspace_bytes': (ct.c_int, [ct.c_int, P]),
     'ehss_trace_blocks': (ct.c_int, [P, ct.c_int, I64, P, P, P, I64, P, U64, P, P]),
+    'ehss_trace_blocks_residual': (ct.c_int, [P, ct.c_int, I64, P, P, P, I64, P, U64, P, P, I64, P, P]),
+    'ehss_extend_blocks': (ct.c_int, [P, ct.c_int, P, ct.c_int, P, I64, ct.c_int, P, P, P, P, I64, P, P, P]),
 }
 
 _LIB = None

@@ -121,7 +121,8 @@ class BatchScenes:
 
 class BatchCCS:
     def __init__(self, structures, log2_rays, seeds, repeats=3, cap=64, precision='fp32', ehss=True, pa=False,
-                 leaf_size=8, launch=None, device=None, graph=True, exterior=True):
+                 leaf_size=8, launch=None, device=None, graph=True, exterior=True, cap_ladder=None,
+                 tail_fraction=5e-4):
         S = len(structures)
         log2s = [int(log2_rays)] * S if np.isscalar(log2_rays) else [int(x) for x in log2_rays]
         seeds = [int(x) for x in (seeds if not np.isscalar(seeds) else [seeds] * S)]
@@ -135,7 +136,11 @@ class BatchCCS:
             for k, seed in enumerate(seed_schedule(sd, repeats)):
                 jobs.append(BlockJob(sc, lg, seed, cap=cap, precision=prec, ehss=ehss, pa=pa, tag=(s, k)))
         self.repeats = int(repeats)
-        self.plan = BlockPlan(jobs, launch=launch, device=self.device)
+        self.cap_ladder = tuple(int(c) for c in cap_ladder) if cap_ladder else ()
+        self.tail_fraction = float(tail_fraction)
+        rays = sum(1 << j.log2_rays for j in jobs)
+        self.plan = BlockPlan(jobs, launch=launch, device=self.device,
+                              residual_capacity=max(4096, rays // 256) if self.cap_ladder else 0)
         self.rays = self.plan.rays
         self.use_graph = graph
         self.h2d_bytes = self.batch.h2d_bytes
@@ -155,6 +160,8 @@ class BatchCCS:
 
     def download(self):
         blocks = self.plan.collect()
+        if self.cap_ladder:
+            blocks = self.plan.extend_caps(self.cap_ladder, self.tail_fraction, results=blocks)
         S, R = len(self.scenes), self.repeats
         out = [dict(structure=s, atoms=sc.n_atoms, runs=blocks[s * R:(s + 1) * R]) for s, sc in enumerate(self.scenes)]
 

@@ -43,7 +43,14 @@ class BlockJob:
 
 
 class BlockPlan:
-    def __init__(self, jobs, launch=None, device=None):
+    """Device descriptors, buffers and the launch for a list of blocks.
+
+    ``residual_capacity`` > 0 saves every ray left unresolved at its block's
+    cap (position, direction, incoming direction, last collider, bounces) so
+    that ``extend_caps`` can continue exactly those rays at larger caps.
+    """
+
+    def __init__(self, jobs, launch=None, device=None, residual_capacity=0):
         if not jobs:
             raise ValueError('at least one block required')
         lib = _lib.load()
@@ -98,14 +105,34 @@ class BlockPlan:
         self.work = t.zeros(int(wb.value) // 8 + 1, dtype=t.int64, device=self.device)
         self.graph = None
         self.rays = sum(1 << j.log2_rays for j in self.jobs)
+        self.residual = None
+        self.residual_capacity = 0
+        self.residual_count = t.zeros(1, dtype=t.int64, device=self.device)
+        if residual_capacity:
+            self._alloc_residual(int(residual_capacity))
+
+    def _alloc_residual(self, capacity):
+        t = torch()
+        self.residual_capacity = max(1, int(capacity))
+        self.residual = t.empty(self.residual_capacity * ct.sizeof(_lib.Residual), dtype=t.uint8, device=self.device)
+        self.graph = None           # a captured launch holds the old buffer
 
     def enqueue(self, stream=None):
         """Enqueue the launch on the current (or given) CUDA stream."""
         lib = _lib.load()
         s = stream_handle(self.device) if stream is None else stream
-        _lib.check(lib.ehss_trace_blocks(ptr(self.blocks_dev), len(self.jobs), self.total_chunks, ptr(self.results),
-                                         ptr(self.hist), ptr(self.ledger), self.hist_entries, ptr(self.work),
-                                         self.work.numel() * 8, ct.byref(self.launch), s), 'trace blocks')
+        if self.residual is None:
+            _lib.check(lib.ehss_trace_blocks(ptr(self.blocks_dev), len(self.jobs), self.total_chunks,
+                                             ptr(self.results), ptr(self.hist), ptr(self.ledger), self.hist_entries,
+                                             ptr(self.work), self.work.numel() * 8, ct.byref(self.launch), s),
+                       'trace blocks')
+        else:
+            _lib.check(lib.ehss_trace_blocks_residual(ptr(self.blocks_dev), len(self.jobs), self.total_chunks,
+                                                      ptr(self.results), ptr(self.hist), ptr(self.ledger),
+                                                      self.hist_entries, ptr(self.work), self.work.numel() * 8,
+                                                      ct.byref(self.launch), ptr(self.residual),
+                                                      self.residual_capacity, ptr(self.residual_count), s),
+                       'trace blocks')
 
     def capture(self):
         """Record the launch (resets + persistent kernel) in a CUDA graph."""
@@ -172,6 +199,104 @@ class BlockPlan:
                 d['pa_blocked_rays'] = pab[i]
             out.append(d)
         return out
+
+
+    def extend_caps(self, caps, tail_fraction=5e-4, results=None):
+        """Cap-extension ladder: continue the unresolved rays of every block
+        whose sampled tail bound exceeds ``tail_fraction`` of its CCS at each
+        cap of ``caps`` in turn (the reference's production rule: 512, then
+        1024, 2048 and 4096 while the bound exceeds 0.05 %).  Only the saved
+        unresolved rays are traced again, from their exact state, so each
+        block's totals equal a run at its final cap.  Returns the block dicts
+        of ``collect`` updated to the final caps, each with ``cap`` and the
+        list ``cap_attempts`` (cap, CCS, tail bound, unresolved and continued
+        rays, seconds)."""
+        import time
+        if self.residual is None:
+            raise ValueError('the plan was built without residual_capacity: nothing was saved to extend')
+        t = torch()
+        lib = _lib.load()
+        res = self.collect() if results is None else results
+        count = int(self.residual_count.item())
+        if count > self.residual_capacity:
+            # the saved rays overflowed: trace again with room for all of them (same results)
+            self._alloc_residual(count)
+            self.enqueue()
+            res = self.collect()
+            count = int(self.residual_count.item())
+        n = len(self.jobs)
+        H, nw = self.hist_len, n * _RESULT_WORDS
+        packed = self.packed.cpu().numpy().view(np.uint64)
+        raw = packed[:nw].reshape(n, _RESULT_WORDS)
+        state = []
+        for i, j in enumerate(self.jobs):
+            o = self._offsets[i]
+            state.append(dict(cap=j.cap, angle_fx=int(raw[i, 0]), escaped=int(raw[i, 3]), unresolved=int(raw[i, 2]),
+                              hist=[int(x) for x in packed[nw + o:nw + o + j.cap + 1]],
+                              ledger=[int(x) for x in packed[nw + H + o:nw + H + o + j.cap + 1]]))
+        attempts = [[dict(cap=j.cap, ehss_angstrom2=r.get('ehss_angstrom2'), tail_bound_angstrom2=r.get(
+            'tail_bound_angstrom2'), unresolved_rays=r.get('unresolved_rays'), continued_rays=0, seconds=0.0)]
+                    for j, r in zip(self.jobs, res)]
+        queue, n_in = self.residual, min(count, self.residual_capacity)
+        stream = stream_handle(self.device)
+        for new_cap in caps:
+            new_cap = int(new_cap)
+            need = [i for i, (j, st) in enumerate(zip(self.jobs, state))
+                    if j.ehss and st['unresolved'] and st['cap'] < new_cap and
+                    2 * self._w[i] * st['unresolved'] > tail_fraction * self._w[i] * st['angle_fx'] * _lib.FX_SCALE]
+            if not need or n_in == 0:
+                break
+            tick = time.perf_counter()
+            rows = len(need)
+            row_of = np.full(n, -1, dtype=np.int32)
+            row_of[need] = np.arange(rows, dtype=np.int32)
+            row_dev = t.from_numpy(row_of).to(self.device)
+            ext = t.zeros(rows * ct.sizeof(_lib.Extension), dtype=t.uint8, device=self.device)
+            eh = t.zeros(rows * (new_cap + 1), dtype=t.int64, device=self.device)
+            el = t.zeros(rows * (new_cap + 1), dtype=t.int64, device=self.device)
+            out = t.empty(max(1, n_in) * ct.sizeof(_lib.Residual), dtype=t.uint8, device=self.device)
+            out_count = t.zeros(1, dtype=t.int64, device=self.device)
+            stats = t.zeros(_lib.NSTATS, dtype=t.int64, device=self.device)
+            _lib.check(lib.ehss_extend_blocks(ptr(self.blocks_dev), n, ptr(row_dev), rows, ptr(queue), n_in, new_cap,
+                                              ptr(ext), ptr(eh), ptr(el), ptr(out), max(1, n_in), ptr(out_count),
+                                              ptr(stats), stream), 'cap extension')
+            e = ext.cpu().numpy().view(np.uint64).reshape(rows, 4)
+            ehh = eh.cpu().numpy().view(np.uint64).reshape(rows, new_cap + 1)
+            ell = el.cpu().numpy().view(np.uint64).reshape(rows, new_cap + 1)
+            st_dev = stats.cpu().numpy()
+            if st_dev[_lib.STAT_ERRORS]:
+                raise _lib.EHSSDeviceError(f'cap extension: {int(st_dev[_lib.STAT_ERRORS])} bounded device failures')
+            secs = time.perf_counter() - tick
+            for r, i in enumerate(need):
+                st = state[i]
+                angle, esc, unres, cont = (int(x) for x in e[r])
+                old = st['cap']
+                st['hist'] += [0] * (new_cap - old)
+                st['ledger'] += [0] * (new_cap - old)
+                st['hist'][old] -= cont
+                for k in range(old, new_cap + 1):
+                    st['hist'][k] += int(ehh[r, k])
+                    st['ledger'][k] += int(ell[r, k])
+                st['angle_fx'] += angle
+                st['escaped'] += esc
+                st['unresolved'] += unres - cont
+                st['cap'] = new_cap
+                w = float(self._w[i])
+                attempts[i].append(dict(cap=new_cap, ehss_angstrom2=w * (st['angle_fx'] * _lib.FX_SCALE),
+                                        tail_bound_angstrom2=2 * w * st['unresolved'],
+                                        unresolved_rays=st['unresolved'], continued_rays=cont, seconds=secs))
+            queue, n_in = out, int(out_count.item())
+        final = []
+        for i, (r, st) in enumerate(zip(res, state)):
+            d = dict(r)
+            w = float(self._w[i])
+            if self.jobs[i].ehss:
+                d.update(ehss_angstrom2=w * (st['angle_fx'] * _lib.FX_SCALE), tail_bound_angstrom2=2 * w * st['unresolved'],
+                         unresolved_rays=st['unresolved'], escaped_rays=st['escaped'], collision_histogram=st['hist'],
+                         collision_contribution_angstrom2=[x * _lib.FX_SCALE * w for x in st['ledger']])
+            d.update(cap=st['cap'], cap_attempts=attempts[i])
+            final.append(d)
+        return final
 
 
 def seed_schedule(seed, repeats):

@@ -272,10 +272,11 @@ int ehss_blocks_workspace_bytes(int n_blocks, uint64_t* bytes) {
     return EHSS_OK;
 }
 
-int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks, ehss_block_result* results_dev,
-                      uint64_t* hist_dev, uint64_t* ledger_dev, int64_t hist_entries, void* workspace_dev,
-                      uint64_t workspace_bytes, const ehss_launch* launch, void* stream) {
-    clear_error();
+static int trace_blocks_impl(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks,
+                             ehss_block_result* results_dev, uint64_t* hist_dev, uint64_t* ledger_dev,
+                             int64_t hist_entries, void* workspace_dev, uint64_t workspace_bytes,
+                             const ehss_launch* launch, ehss_residual* residual_dev, int64_t residual_capacity,
+                             unsigned long long* residual_count_dev, void* stream) {
     if (!blocks_dev || n_blocks < 1 || !results_dev || !hist_dev || !ledger_dev || !workspace_dev || !launch) {
         set_error("invalid arguments");
         return EHSS_ERR_VALUE;
@@ -304,9 +305,59 @@ int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_
     if (!rc) rc = cuda_status(cudaMemsetAsync(workspace_dev, 0, sizeof(unsigned long long) * kMaxWorkParts, s),
                               "work counter reset");
     if (rc) return rc;
+    if (residual_count_dev) {
+        rc = cuda_status(cudaMemsetAsync(residual_count_dev, 0, sizeof(unsigned long long), s), "residual count reset");
+        if (rc) return rc;
+    }
     if (total_chunks == 0) return EHSS_OK;
     return launch_blocks(blocks_dev, n_blocks, total_chunks, L, results_dev, hist_dev, ledger_dev,
-                         reinterpret_cast<unsigned long long*>(workspace_dev), s);
+                         reinterpret_cast<unsigned long long*>(workspace_dev), s, residual_dev, residual_capacity,
+                         residual_count_dev);
+}
+
+int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks, ehss_block_result* results_dev,
+                      uint64_t* hist_dev, uint64_t* ledger_dev, int64_t hist_entries, void* workspace_dev,
+                      uint64_t workspace_bytes, const ehss_launch* launch, void* stream) {
+    clear_error();
+    return trace_blocks_impl(blocks_dev, n_blocks, total_chunks, results_dev, hist_dev, ledger_dev, hist_entries,
+                             workspace_dev, workspace_bytes, launch, nullptr, 0, nullptr, stream);
+}
+
+int ehss_trace_blocks_residual(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks,
+                               ehss_block_result* results_dev, uint64_t* hist_dev, uint64_t* ledger_dev,
+                               int64_t hist_entries, void* workspace_dev, uint64_t workspace_bytes,
+                               const ehss_launch* launch, ehss_residual* residual_dev, int64_t residual_capacity,
+                               unsigned long long* residual_count_dev, void* stream) {
+    clear_error();
+    if (!residual_dev || residual_capacity < 1 || !residual_count_dev) {
+        set_error("residual buffer, capacity >= 1 and count pointer required");
+        return EHSS_ERR_VALUE;
+    }
+    return trace_blocks_impl(blocks_dev, n_blocks, total_chunks, results_dev, hist_dev, ledger_dev, hist_entries,
+                             workspace_dev, workspace_bytes, launch, residual_dev, residual_capacity,
+                             residual_count_dev, stream);
+}
+
+int ehss_extend_blocks(const ehss_block* blocks_dev, int n_blocks, const int32_t* row_dev, int rows,
+                       const ehss_residual* in_dev, int64_t n_in, int new_cap, ehss_extension* ext_dev,
+                       uint64_t* hist_dev, uint64_t* ledger_dev, ehss_residual* out_dev, int64_t out_capacity,
+                       unsigned long long* out_count_dev, uint64_t* stats_dev, void* stream) {
+    clear_error();
+    if (!blocks_dev || n_blocks < 1 || !row_dev || rows < 1 || n_in < 0 || (n_in > 0 && !in_dev) || !ext_dev ||
+        !hist_dev || !ledger_dev || !out_dev || out_capacity < 1 || !out_count_dev) {
+        set_error("invalid arguments");
+        return EHSS_ERR_VALUE;
+    }
+    if (new_cap < 2 || new_cap > 100000) { set_error("new_cap must be 2..100000"); return EHSS_ERR_VALUE; }
+    cudaStream_t s = as_stream(stream);
+    const size_t per = (size_t)(new_cap + 1) * (size_t)rows;
+    int rc = cuda_status(cudaMemsetAsync(ext_dev, 0, sizeof(ehss_extension) * (size_t)rows, s), "extension reset");
+    if (!rc) rc = cuda_status(cudaMemsetAsync(hist_dev, 0, 8 * per, s), "extension hist reset");
+    if (!rc) rc = cuda_status(cudaMemsetAsync(ledger_dev, 0, 8 * per, s), "extension ledger reset");
+    if (!rc) rc = cuda_status(cudaMemsetAsync(out_count_dev, 0, sizeof(unsigned long long), s), "residual count reset");
+    if (rc) return rc;
+    return launch_extend(blocks_dev, n_blocks, row_dev, rows, in_dev, n_in, new_cap, ext_dev, hist_dev, ledger_dev,
+                         out_dev, out_capacity, out_count_dev, stats_dev, s);
 }
 
 }  // extern "C"

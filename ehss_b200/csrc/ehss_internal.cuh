@@ -58,6 +58,7 @@ struct alignas(256) SceneHeader {
     uint64_t bytes;
 };
 static_assert(sizeof(SceneHeader) == 256, "scene header is one 256-byte line");
+static_assert(sizeof(ehss_residual) == 88 && offsetof(ehss_residual, block) == 72, "residual ray record layout");
 static_assert(sizeof(ehss_block) % 16 == 0 && offsetof(ehss_block, basis) == 0 && offsetof(ehss_block, base) == 480,
               "block descriptors are read with 16-byte vector loads");
 
@@ -241,8 +242,13 @@ int launch_source_rays(const void* scene, const Sobol4Params& p, int64_t first, 
 uint64_t grid_workspace_bytes(int64_t n_atoms, int n_dirs, int n);
 int launch_grid_pa(const void* scene, int64_t n_atoms, int n_dirs, uint64_t seed, int n, unsigned long long* counts,
                    double* spacing_out, double* xy_out, void* workspace, uint64_t ws_bytes, cudaStream_t stream);
+int launch_extend(const ehss_block* blocks, int nb, const int32_t* row, int rows, const ehss_residual* in,
+                  int64_t n_in, int new_cap, ehss_extension* ext, uint64_t* hist, uint64_t* ledger,
+                  ehss_residual* out, int64_t out_capacity, unsigned long long* out_count, uint64_t* stats,
+                  cudaStream_t stream);
 int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const ehss_launch& L,
                   ehss_block_result* results, uint64_t* hist, uint64_t* ledger, unsigned long long* work,
-                  cudaStream_t stream);
+                  cudaStream_t stream, ehss_residual* residual = nullptr, int64_t residual_capacity = 0,
+                  unsigned long long* residual_count = nullptr);
 
 }  // namespace ehss

@@ -631,6 +631,19 @@ __device__ __forceinline__ int resolve_candidates(const SceneView& S, const Walk
     return k;
 }
 
+// Rare path of k_blocks, kept out of line so that it costs the hot loop no registers.
+__device__ __noinline__ void save_residual(ehss_residual* residual, long long capacity, unsigned long long* count,
+                                           const LaneRay& L, int block, int last_rank, int bounces) {
+    unsigned long long at = atomicAdd(count, 1ull);
+    if (at >= (unsigned long long)capacity) return;
+    ehss_residual& R = residual[at];
+    for (int i = 0; i < 3; ++i) { R.o[i] = L.o[i]; R.d[i] = L.d[i]; R.din[i] = L.din[i]; }
+    R.block = block;
+    R.last_rank = last_rank;
+    R.bounces = bounces;
+    R.reserved = 0;
+}
+
 // Work distribution: the chunk list is cut into one contiguous range per SM
 // (partition = %smid mod n_parts) so that the warps of an SM trace the same
 // structure, and neighbouring regions of its ray space, at the same time and
@@ -654,7 +667,8 @@ template <bool EXACT, bool COUNT>
 __global__ void __launch_bounds__(128, 6) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
                                                    int chunk_rays, int resolve_batch, ehss_block_result* results,
                                                    uint64_t* hist, uint64_t* ledger, unsigned long long* work,
-                                                   int n_parts, int smem_stack) {
+                                                   int n_parts, int smem_stack, ehss_residual* residual,
+                                                   long long residual_capacity, unsigned long long* residual_count) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     WarpAcc& A = reinterpret_cast<WarpAcc*>(smem_raw)[warp];
@@ -732,6 +746,8 @@ __global__ void __launch_bounds__(128, 6) k_blocks(const ehss_block* blocks, int
                         if (fx) atomicAdd(&A.angle_fx, fx);
                     } else {
                         atomicAdd(&A.unresolved, 1u);
+                        // save the state for a later cap extension
+                        if (residual) save_residual(residual, residual_capacity, residual_count, L, bi, last_rank, bounces);
                     }
                     if (bounces > 0 || !escaped) atomicAdd(&A.hits, 1u);
                     if (bounces < kSmemBins) {
@@ -882,7 +898,8 @@ int launch_source_rays(const void* scene, const Sobol4Params& p, int64_t first, 
 
 int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const ehss_launch& L,
                   ehss_block_result* results, uint64_t* hist, uint64_t* ledger, unsigned long long* work,
-                  cudaStream_t stream) {
+                  cudaStream_t stream, ehss_residual* residual, int64_t residual_capacity,
+                  unsigned long long* residual_count) {
     int warps = L.block_threads / 32;
     const int sdepth = L.smem_stack > 0 ? L.smem_stack : 16;
     size_t smem = sizeof(WarpAcc) * (size_t)warps + sizeof(LaneRay) * (size_t)L.block_threads +
@@ -904,7 +921,8 @@ int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const 
         const int n_parts = sm_count() < kMaxWorkParts ? sm_count() : kMaxWorkParts;
 #define EHSS_LAUNCH_BLOCKS(E, C) \
         k_blocks<E, C><<<grid, L.block_threads, smem, stream>>>(blocks, nb, total_chunks, L.chunk_rays, batch, \
-                                                                results, hist, ledger, work, n_parts, sdepth)
+                                                                results, hist, ledger, work, n_parts, sdepth, \
+                                                                residual, residual_capacity, residual_count)
         if (exact) { if (count) EHSS_LAUNCH_BLOCKS(true, true); else EHSS_LAUNCH_BLOCKS(true, false); }
         else { if (count) EHSS_LAUNCH_BLOCKS(false, true); else EHSS_LAUNCH_BLOCKS(false, false); }
 #undef EHSS_LAUNCH_BLOCKS
@@ -912,6 +930,90 @@ int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const 
         if (rc) return rc;
     }
     return EHSS_OK;
+}
+
+// --------------------------------------------------------------------------
+// Cap extension: continue saved unresolved rays (one thread per ray) from
+// their exact state, so each follows the path it would have followed with
+// the larger cap from the start.  Sums are the same integers k_blocks uses.
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_extend(const ehss_block* blocks, int nb, const int32_t* row_of, int rows,
+                                                const ehss_residual* in, int64_t n_in, int new_cap,
+                                                ehss_extension* ext, uint64_t* hist, uint64_t* ledger,
+                                                ehss_residual* out, int64_t out_capacity,
+                                                unsigned long long* out_count, uint64_t* stats) {
+    LocalStats st;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_in; i += stride) {
+        const ehss_residual R = in[i];
+        if (R.block < 0 || R.block >= nb) { ++st.errors; continue; }
+        const int row = row_of[R.block];
+        if (row < 0) continue;
+        if (row >= rows) { ++st.errors; continue; }
+        const ehss_block* B = blocks + R.block;
+        const SceneView S = scene_view(B->scene);
+        if (S.h->magic != kSceneMagic || S.h->status != 0 || R.bounces >= new_cap || R.last_rank < -1 ||
+            R.last_rank >= S.h->n_atoms) {
+            ++st.errors;
+            continue;
+        }
+        const bool exact = B->precision == EHSS_PREC_FP64;
+        double o[3] = {R.o[0], R.o[1], R.o[2]}, d[3] = {R.d[0], R.d[1], R.d[2]};
+        int last_rank = R.last_rank, count = R.bounces;
+        bool escaped = false;
+        double so[3], sd[3];
+        int s_last = last_rank;
+        while (true) {
+            double best;
+            const int k = exact ? nearest<true>(S, o, d, last_rank, best, st) : nearest<false>(S, o, d, last_rank, best, st);
+            if (k < 0) { escaped = true; break; }
+            if (count >= new_cap) {
+                for (int c = 0; c < 3; ++c) { so[c] = o[c]; sd[c] = d[c]; }
+                s_last = last_rank;
+                break;
+            }
+            const double4 a = S.atoms64[k];
+            reflect64(o[0], o[1], o[2], d[0], d[1], d[2], a.x, a.y, a.z, a.w, best);
+            ++count;
+            last_rank = k;
+        }
+        ehss_extension& E = ext[row];
+        uint64_t* h = hist + (int64_t)row * (new_cap + 1);
+        uint64_t* l = ledger + (int64_t)row * (new_cap + 1);
+        atomicAdd((unsigned long long*)&E.continued, 1ull);
+        atomicAdd((unsigned long long*)&h[count], 1ull);
+        if (escaped) {
+            const double ang = scatter_angle(R.din[0], R.din[1], R.din[2], d[0], d[1], d[2]);
+            const unsigned long long fx = __double2ull_rn(ang * 0x1p40);
+            atomicAdd((unsigned long long*)&E.escaped, 1ull);
+            if (fx) {
+                atomicAdd((unsigned long long*)&E.angle_fx, fx);
+                atomicAdd((unsigned long long*)&l[count], fx);
+            }
+        } else {
+            atomicAdd((unsigned long long*)&E.unresolved, 1ull);
+            const unsigned long long at = atomicAdd(out_count, 1ull);
+            if (at < (unsigned long long)out_capacity) {
+                ehss_residual& Q = out[at];
+                for (int c = 0; c < 3; ++c) { Q.o[c] = so[c]; Q.d[c] = sd[c]; Q.din[c] = R.din[c]; }
+                Q.block = R.block;
+                Q.last_rank = s_last;
+                Q.bounces = count;
+                Q.reserved = 0;
+            }
+        }
+    }
+    flush_stats(st, stats);
+}
+
+int launch_extend(const ehss_block* blocks, int nb, const int32_t* row, int rows, const ehss_residual* in,
+                  int64_t n_in, int new_cap, ehss_extension* ext, uint64_t* hist, uint64_t* ledger,
+                  ehss_residual* out, int64_t out_capacity, unsigned long long* out_count, uint64_t* stats,
+                  cudaStream_t stream) {
+    if (n_in == 0) return EHSS_OK;
+    k_extend<<<grid_for(n_in, 128), 128, 0, stream>>>(blocks, nb, row, rows, in, n_in, new_cap, ext, hist, ledger,
+                                                      out, out_capacity, out_count, stats);
+    return cuda_status(cudaGetLastError(), "cap extension launch");
 }
 
 }  // namespace ehss

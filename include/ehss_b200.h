@@ -269,6 +269,55 @@ int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_
                       int64_t hist_entries, void* workspace_dev, uint64_t workspace_bytes,
                       const ehss_launch* launch, void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Cap extension.  The reference's production runs start at cap 512 and
+ * retrace the same rays at caps 1024, 2048 and 4096 while a run's sampled
+ * tail bound exceeds 0.05 % of its CCS (manuscript, Methods; the wrapper
+ * itself is not in the reference tree).  Here the rays left unresolved at a
+ * block's cap are saved with their full state, and only they are continued:
+ * a ray continued from its saved state follows the path it would have
+ * followed with the larger cap from the start, so merged totals equal a run
+ * at the larger cap, bit for bit. */
+typedef struct ehss_residual {
+    double o[3];          /* last bounce point */
+    double d[3];          /* direction leaving it */
+    double din[3];        /* the ray's incoming direction */
+    int32_t block;        /* index of its block in the blocks array */
+    int32_t last_rank;    /* leaf-order index of the last collider */
+    int32_t bounces;      /* collisions so far (the cap it stopped at) */
+    int32_t reserved;
+} ehss_residual;
+
+typedef struct ehss_extension {   /* one row per extended block */
+    uint64_t angle_fx;    /* angle sum (2^-40 units) of the continued rays that escaped */
+    uint64_t escaped;     /* continued rays that escaped */
+    uint64_t unresolved;  /* continued rays still unresolved at the new cap */
+    uint64_t continued;   /* continued rays */
+} ehss_extension;
+
+/* ehss_trace_blocks that also appends every ray left unresolved to
+ * residual_dev[0 .. residual_capacity) and counts them in
+ * *residual_count_dev (zeroed by the call; a count above the capacity means
+ * the extra rays were not saved). */
+int ehss_trace_blocks_residual(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks,
+                               ehss_block_result* results_dev, uint64_t* hist_dev, uint64_t* ledger_dev,
+                               int64_t hist_entries, void* workspace_dev, uint64_t workspace_bytes,
+                               const ehss_launch* launch, ehss_residual* residual_dev, int64_t residual_capacity,
+                               unsigned long long* residual_count_dev, void* stream);
+
+/* Continue saved rays to new_cap.  row_dev[n_blocks] (device int32) maps a
+ * block to its row in ext_dev / hist_dev / ledger_dev, or -1 to leave that
+ * block's rays alone.  ext_dev[rows] and hist_dev/ledger_dev[rows *
+ * (new_cap + 1)] are zeroed by the call; a continued ray that escapes adds
+ * its angle to its row and counts at hist[row * (new_cap + 1) + bounces], one
+ * still unresolved counts at bounces = new_cap and is appended to out_dev
+ * (count in *out_count_dev, zeroed by the call).  new_cap must exceed the
+ * bounce count of every continued ray.  stats_dev: NULL or uint64[EHSS_NSTATS]. */
+int ehss_extend_blocks(const ehss_block* blocks_dev, int n_blocks, const int32_t* row_dev, int rows,
+                       const ehss_residual* in_dev, int64_t n_in, int new_cap, ehss_extension* ext_dev,
+                       uint64_t* hist_dev, uint64_t* ledger_dev, ehss_residual* out_dev, int64_t out_capacity,
+                       unsigned long long* out_count_dev, uint64_t* stats_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -120,3 +120,52 @@ def test_exterior_scene_refused_for_explicit_rays(eb):
     _lib.check(_lib.load().ehss_pa_anyhit(sc.ptr, n, o.data_ptr(), d.data_ptr(), own.data_ptr(), blocked.data_ptr(),
                                           stats.data_ptr(), torch.cuda.current_stream().cuda_stream))
     assert int(stats[_lib.STAT_ERRORS]) == n and int(blocked.sum()) == 0
+
+
+def _padded(d, cap):
+    h = list(d['collision_histogram']) + [0] * (cap + 1 - len(d['collision_histogram']))
+    l = list(d['collision_contribution_angstrom2']) + [0.0] * (cap + 1 - len(d['collision_contribution_angstrom2']))
+    return h, l
+
+
+@pytest.mark.parametrize('precision,capacity', [('fp64', 1 << 16), ('fp32', 1 << 16), ('fp32', 3)])
+def test_cap_extension_equals_a_run_at_the_larger_cap(eb, precision, capacity):
+    """Continuing only the saved unresolved rays gives the totals of a run
+    that used the larger cap from the start (capacity 3 forces the re-trace
+    with a larger residual buffer)."""
+    from ehss_b200 import _lib
+    from ehss_b200.blocks import BlockJob, BlockPlan
+    prec = {'fp64': _lib.PREC_FP64, 'fp32': _lib.PREC_FP32}[precision]
+    scenes = [eb.Scene(c, r, exterior=True) for c, r in _structures([300, 1800], seed=41)]
+    jobs = lambda cap: [BlockJob(sc, 12, 100 + k, cap=cap, precision=prec, pa=True, tag=(s, k))
+                        for s, sc in enumerate(scenes) for k in range(2)]
+    plan = BlockPlan(jobs(3), residual_capacity=capacity)
+    plan.run()
+    first = plan.collect()
+    assert sum(r['unresolved_rays'] for r in first) > 10
+    ext = plan.extend_caps((6, 12, 64), tail_fraction=0.0)
+    ref = BlockPlan(jobs(64))
+    ref.run()
+    full = ref.collect()
+    for a, b, f in zip(ext, full, first):
+        for key in ('ehss_angstrom2', 'tail_bound_angstrom2', 'unresolved_rays', 'escaped_rays',
+                    'pa_from_same_rays_angstrom2', 'pa_angstrom2'):
+            assert a[key] == b[key], key
+        assert _padded(a, 64) == _padded(b, 64)
+        caps = [x['cap'] for x in a['cap_attempts']]
+        assert caps[0] == 3 and caps == sorted(caps) and a['cap'] == caps[-1]
+        assert a['cap'] == 64 or a['unresolved_rays'] == 0
+        assert sum(x['continued_rays'] for x in a['cap_attempts'][1:2]) == f['unresolved_rays']
+
+
+def test_batchccs_cap_ladder_stops_when_the_tail_is_small(eb):
+    from ehss_b200.batch import BatchCCS
+    structures = _structures([200, 900], seed=43)
+    low = BatchCCS(structures, 12, [1, 2], repeats=2, cap=4, cap_ladder=(8, 16, 64), tail_fraction=5e-4, graph=False)
+    out = low.run()
+    for o in out:
+        for run in o['runs']:
+            att = run['cap_attempts']
+            last = att[-1]
+            assert last['tail_bound_angstrom2'] <= 5e-4 * last['ehss_angstrom2'] or last['cap'] == 64
+            assert all(x['tail_bound_angstrom2'] > 5e-4 * x['ehss_angstrom2'] for x in att[:-1])
