@@ -54,6 +54,11 @@ class Extension(ct.Structure):
     _fields_ = [('angle_fx', U64), ('escaped', U64), ('unresolved', U64), ('continued', U64)]
 
 
+class Boundary(ct.Structure):
+    _fields_ = [('kind', I32), ('reserved', I32), ('center', ct.c_double * 3), ('rotation', ct.c_double * 9),
+                ('axes', ct.c_double * 3)]
+
+
 class Launch(ct.Structure):
     _fields_ = [('block_threads', I32), ('ctas_per_sm', I32), ('chunk_rays', I32), ('resolve_batch', I32),
                 ('precisions', I32), ('options', I32), ('smem_stack', I32), ('reserved', I32)]
@@ -72,6 +77,7 @@ _SIGNATURES = {
     'ehss_scenes_build_ex': (ct.c_int, [ct.c_int, P, P, P, ct.c_int, P, P, P, U64, ct.c_uint32, P]),
     'ehss_scene_info_get': (ct.c_int, [P, P, P]),
     'ehss_source_rays': (ct.c_int, [P, ct.c_int, U64, I64, I64, P, P, P]),
+    'ehss_compact_source_rays': (ct.c_int, [P, ct.c_int, U64, I64, I64, P, P, P, P]),
     'ehss_trace': (ct.c_int, [P, I64, ct.c_int, ct.c_int, P, P, P, P, P, P, P, P, P]),
     'ehss_pa_anyhit': (ct.c_int, [P, I64, P, P, P, P, P, P]),
     'ehss_pa_grid_workspace_bytes': (ct.c_int, [I64, ct.c_int, ct.c_int, P]),

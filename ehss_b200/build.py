@@ -18,7 +18,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / 'csrc'
 ROOT = HERE.parent
 LIB = HERE / 'libehss_b200.so'
-SOURCES = ['capi.cu', 'scene.cu', 'trace.cu', 'pa_grid.cu', 'noalloc.cu', 'sobol_host.cpp']
+SOURCES = ['capi.cu', 'scene.cu', 'trace.cu', 'pa_grid.cu', 'compact.cu', 'noalloc.cu', 'sobol_host.cpp']
 HEADERS = ['ehss_internal.cuh']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 

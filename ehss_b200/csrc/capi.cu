@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cmath>
 #include "ehss_internal.cuh"
 
 namespace ehss {
@@ -79,6 +80,33 @@ int ehss_sobol_points(int dim, uint64_t seed, int64_t first, int64_t n, uint32_t
     memset(&p, 0, sizeof(p));
     sobol_scramble(dim, seed, p.sv, p.shift);
     return launch_sobol_points(dim, p, first, n, q_dev, as_stream(stream));
+}
+
+int ehss_compact_source_rays(const ehss_boundary* boundary_host, int log2n, uint64_t seed, int64_t first, int64_t n,
+                             double* origins_dev, double* directions_dev, double* weights_dev, void* stream) {
+    clear_error();
+    if (!boundary_host) { set_error("null boundary"); return EHSS_ERR_VALUE; }
+    const ehss_boundary& B = *boundary_host;
+    if (B.kind != EHSS_BOUNDARY_SPHERE && B.kind != EHSS_BOUNDARY_ELLIPSOID && B.kind != EHSS_BOUNDARY_BOX) {
+        set_error("Boundary must be sphere, ellipsoid, or box");
+        return EHSS_ERR_VALUE;
+    }
+    for (int k = 0; k < 3; ++k)
+        if (!(B.axes[k] > 0.) || !std::isfinite(B.axes[k]) || !std::isfinite(B.center[k])) {
+            set_error("boundary centre must be finite and its semi-axes positive and finite");
+            return EHSS_ERR_VALUE;
+        }
+    for (int k = 0; k < 9; ++k)
+        if (!std::isfinite(B.rotation[k])) { set_error("boundary rotation must be finite"); return EHSS_ERR_VALUE; }
+    if (log2n < 0 || log2n > 30) { set_error("log2n must be 0..30"); return EHSS_ERR_VALUE; }
+    if (first < 0 || n < 0 || first + n > (1ll << log2n)) { set_error("ray range outside the sequence"); return EHSS_ERR_VALUE; }
+    if (n > 0 && (!origins_dev || !directions_dev || !weights_dev)) { set_error("null output pointer"); return EHSS_ERR_VALUE; }
+    const int dim = B.kind == EHSS_BOUNDARY_BOX ? 5 : 4;
+    SobolParams p;
+    memset(&p, 0, sizeof(p));
+    sobol_scramble(dim, seed, p.sv, p.shift);
+    return launch_compact_rays(B, p, dim, first, n, 1.0 / (double)(1ll << log2n), origins_dev, directions_dev,
+                               weights_dev, as_stream(stream));
 }
 
 int ehss_scene_bytes(int64_t n_atoms, int leaf_size, uint64_t* scene_bytes, uint64_t* workspace_bytes) {

@@ -242,6 +242,8 @@ int launch_source_rays(const void* scene, const Sobol4Params& p, int64_t first, 
 uint64_t grid_workspace_bytes(int64_t n_atoms, int n_dirs, int n);
 int launch_grid_pa(const void* scene, int64_t n_atoms, int n_dirs, uint64_t seed, int n, unsigned long long* counts,
                    double* spacing_out, double* xy_out, void* workspace, uint64_t ws_bytes, cudaStream_t stream);
+int launch_compact_rays(const ehss_boundary& B, const SobolParams& p, int dim, int64_t first, int64_t n,
+                        double inv_count, double* O, double* D, double* W, cudaStream_t stream);
 int launch_extend(const ehss_block* blocks, int nb, const int32_t* row, int rows, const ehss_residual* in,
                   int64_t n_in, int new_cap, ehss_extension* ext, uint64_t* hist, uint64_t* ledger,
                   ehss_residual* out, int64_t out_capacity, unsigned long long* out_count, uint64_t* stats,

@@ -205,9 +205,15 @@ class PreparedStaticGPUEHSS:
         scene = Scene.from_spheres(s, leaf_size=min(leaf_size, 16), device=device)
         self.model = SimpleNamespace(spheres=s, scene=scene)
         self.scene = scene
+        tick = time.perf_counter()
+        from .compact import CompactBoundary
+        # incidence boundary, as the reference's prepared engine carries it (ehss_static.py:94)
+        self.boundary = CompactBoundary.fit(s, boundary, device=scene.device)
+        boundary_s = time.perf_counter() - tick
         self.engine = GPUEHSSTransport(scene, precision=precision, threads=threads)
         self.setup = dict(total_s=time.perf_counter() - start, preparation='static device LBVH',
-                          nodes=int(scene.info.n_nodes), depth=int(scene.info.depth), threads=threads)
+                          nodes=int(scene.info.n_nodes), depth=int(scene.info.depth), threads=threads,
+                          boundary_s=boundary_s)
 
 
 class SphereIndex:

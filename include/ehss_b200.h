@@ -153,6 +153,29 @@ int ehss_source_rays(const void* scene_dev, int log2n, uint64_t seed, int64_t fi
                      double* origins_dev, double* directions_dev, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Incidence on a compact enclosing boundary.  Replaces CompactBoundary.source
+ * (src/support_exchange_transport/ehss_compact_source.py:47-87): directions
+ * uniform on S2 from Sobol dimensions 0-1; origins uniform over the
+ * boundary's projection perpendicular to the direction, upstream of the
+ * boundary (Sobol dimensions 2-3, and 4 for the box); weight = projected
+ * area / 2^log2n.  The boundary (centre, rotation, semi-axes) is the one
+ * CompactBoundary.fit computes (ehss_compact_source.py:24-45); the sphere
+ * boundary is the impact disk of ehss_source_rays.  Writes origins and
+ * directions [n*3] and weights [n] (float64) for ray indices [first, first+n). */
+#define EHSS_BOUNDARY_SPHERE 0
+#define EHSS_BOUNDARY_ELLIPSOID 1
+#define EHSS_BOUNDARY_BOX 2
+typedef struct ehss_boundary {
+    int32_t kind;             /* EHSS_BOUNDARY_* */
+    int32_t reserved;
+    double center[3];
+    double rotation[9];       /* row major; columns are the local axes */
+    double axes[3];           /* semi-axes (sphere: radius in axes[0]) */
+} ehss_boundary;
+int ehss_compact_source_rays(const ehss_boundary* boundary_host, int log2n, uint64_t seed, int64_t first, int64_t n,
+                             double* origins_dev, double* directions_dev, double* weights_dev, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* EHSS trace of explicit rays.  Replaces the reference's native entry point
  * ehss_trace (src/native/ehss_cpu.cpp:42-82) and CPUEHSSTransport.trace
  * (ehss_cpu.py:118-142): positions_dev/directions_dev [n*3] hold the source

@@ -14,8 +14,10 @@ it.  It restates the SCIMMS/EHSS reference's FP64 CPU algorithm:
   scaled by 2**-30.  Direction numbers are the published Joe--Kuo
   (new-joe-kuo-6.21201) values;
 * the impact-disk source (``ehss_state.external_source``, ehss_state.py:42-53;
-  ``unit_sphere``/``tangent_frames``, inside_out_pa.py:45-58) in numpy, which
-  is the same arithmetic the reference performs;
+  ``unit_sphere``/``tangent_frames``, inside_out_pa.py:45-58) and the
+  compact-boundary sources (``CompactBoundary.source``,
+  ehss_compact_source.py:47-87) in numpy, which is the same arithmetic the
+  reference performs;
 * the static BVH, nearest-entry trace and any-hit PA in ``ehss_oracle.c``
   (see that file for per-function citations), loaded through ctypes;
 * the readout (``EHSSResult``, ehss_state.py:84-108; ``ccs_cli.solve_frame``
@@ -150,6 +152,53 @@ def map_impact_disk(u, centers, radii):
 
 def external_source(centers, radii, power, seed):
     return map_impact_disk(sobol_points(4, power, seed), np.asarray(centers, float), np.asarray(radii, float))
+
+
+def compact_source(kind, center, rotation, axes, u):
+    """Rays of an enclosing boundary from Sobol points u[n, 4 or 5]
+    (CompactBoundary.source, ehss_compact_source.py:47-87): directions
+    uniform on S2, origins uniform over the boundary's projection, upstream
+    of it, weight = projected area / n."""
+    center, rotation, axes = (np.asarray(x, dtype=np.float64) for x in (center, rotation, axes))
+    d = unit_sphere(u[:, :2])
+    n = len(d)
+    if kind == 'sphere':
+        t, b = tangent_frames(d)
+        radius = axes[0]
+        rho, phi = radius * np.sqrt(u[:, 2]), 2 * np.pi * u[:, 3]
+        origins = center - radius * d + rho[:, None] * (np.cos(phi)[:, None] * t + np.sin(phi)[:, None] * b)
+        area = np.full(n, np.pi * radius * radius)
+    elif kind == 'box':
+        local_d = d @ rotation
+        face_areas = 4 * np.prod(axes) / axes
+        projected = np.abs(local_d) * face_areas
+        area = projected.sum(axis=1)
+        # face k with probability projected[k] / area (u[:, 2] against the running sums)
+        face = (u[:, 2, None] * area[:, None] >= np.cumsum(projected, axis=1)).sum(axis=1)
+        p = np.empty((n, 3))
+        for axis in range(3):
+            sel = face == axis
+            p[sel, axis] = -np.sign(local_d[sel, axis]) * axes[axis]
+            other = [k for k in range(3) if k != axis]
+            p[np.ix_(sel, other)] = (2 * u[sel, 3:5] - 1) * axes[other]
+        origins = center + p @ rotation.T - 1e-10 * max(1., axes.max()) * d
+    elif kind == 'ellipsoid':
+        t, b = tangent_frames(d)
+        lt, lb = (t @ rotation) * axes, (b @ rotation) * axes
+        g00, g01, g11 = np.sum(lt * lt, axis=1), np.sum(lt * lb, axis=1), np.sum(lb * lb, axis=1)
+        l00 = np.sqrt(g00)
+        l10 = g01 / l00
+        l11 = np.sqrt(np.maximum(0., g11 - l10 * l10))
+        rho, phi = np.sqrt(u[:, 2]), 2 * np.pi * u[:, 3]
+        x, y = rho * np.cos(phi), rho * np.sin(phi)
+        offset = (l00 * x)[:, None] * t + (l10 * x + l11 * y)[:, None] * b
+        extent = np.linalg.norm((d @ rotation) * axes, axis=1)
+        origins = center + offset - (extent * (1 + 1e-10))[:, None] * d
+        area = np.pi * l00 * l11
+    else:
+        raise ValueError('Boundary must be sphere, ellipsoid, or box')
+    return dict(origins=origins, directions=d, incoming=d.copy(), weights=area / n,
+                last_atom=np.full(n, -1, dtype=np.int64), initial_bounces=np.zeros(n, dtype=np.int64))
 
 
 # --------------------------------------------------------------------------

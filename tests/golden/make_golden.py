@@ -40,9 +40,36 @@ def trim_history(h, bounces):
     return np.ascontiguousarray(h[:, :width])
 
 
+def compact_fixtures(Spheres):
+    """Enclosing-boundary fits and their incidence sources (ehss_compact_source.py)."""
+    from support_exchange_transport.ehss_compact_source import CompactBoundary
+    comp = {}
+    structures = [('cloud37', Spheres(*cloud(317, 37, 3, .7, 1.5))), ('cloud300', Spheres(*cloud(4242, 300, 6, 2.5, 3.2))),
+                  ('tri', Spheres(*triatomic(), deduplicate=False)),
+                  ('line', Spheres(np.array([[0., 0., 0.], [1.5, 0., 0.], [3., 0., 0.]]), np.array([1.7, 1.2, 1.7]))),
+                  ('single', Spheres(np.zeros((1, 3)), np.array([3.1])))]
+    for name, s in structures:
+        comp[name + '_centers'] = s.centers
+        comp[name + '_radii'] = s.radii
+        for kind in ('sphere', 'ellipsoid', 'box'):
+            b = CompactBoundary.fit(s, kind)
+            comp[f'{name}_{kind}_center'] = b.center
+            comp[f'{name}_{kind}_rotation'] = b.rotation
+            comp[f'{name}_{kind}_axes'] = b.axes
+            for m, seed in [(6, 11), (9, 190003)]:
+                e = b.source(m, seed)
+                key = f'{name}_{kind}_{m}_{seed}'
+                comp[key + '_origins'] = e.origins
+                comp[key + '_directions'] = e.directions
+                comp[key + '_weights'] = e.weights
+    np.savez_compressed(HERE / 'compact.npz', **comp)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--only', choices=['compact'], default=None,
+                    help='regenerate one fixture file only (the others stay as they are)')
     args = ap.parse_args()
     sys.path.insert(0, str(Path(args.reference) / 'src'))
     from scipy.stats import qmc
@@ -52,6 +79,10 @@ def main():
     from support_exchange_transport.ehss_reference import trace as flat_trace
     from support_exchange_transport.pa_spatial import SphereIndex
     from support_exchange_transport import ccs_cli
+    if args.only == 'compact':
+        compact_fixtures(Spheres)
+        print('wrote compact.npz')
+        return
 
     # ---- Sobol -------------------------------------------------------------
     sob = {}
@@ -207,6 +238,7 @@ def main():
         cli[name] = dict(argv=argv, centers=s.centers.tolist(), radii=s.radii.tolist(),
                          summary=out['summary'], runs=strip(out['runs']))
     (HERE / 'cli.json').write_text(json.dumps(cli, indent=1) + '\n')
+    compact_fixtures(Spheres)
     print('wrote', sorted(p.name for p in HERE.glob('*.npz')), 'cli.json')
 
 

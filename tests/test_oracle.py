@@ -170,3 +170,24 @@ def test_adaptive_pa_bit_exact(golden, name):
     # the union count from the reference's own projected coordinates
     for xy, sp, c in zip(g[name + '_xy'], g[name + '_spacings'], g[name + '_counts']):
         assert O.union_count(xy, g[name + '_radii'], np.array([-sp * grid / 2] * 2), sp, grid) == c
+
+
+def test_compact_sources_and_fits_match_reference():
+    """Oracle compact-boundary sources on scipy-identical Sobol points, and the
+    package's host fit (CompactBoundary.fit), against the reference's own."""
+    import types
+    from ehss_b200.compact import CompactBoundary
+    g = np.load(GOLDEN / 'compact.npz')
+    for name in ('cloud37', 'cloud300', 'tri', 'line', 'single'):
+        s = types.SimpleNamespace(centers=g[name + '_centers'], radii=g[name + '_radii'])
+        for kind in ('sphere', 'ellipsoid', 'box'):
+            b = CompactBoundary.fit(s, kind)
+            np.testing.assert_array_equal(b.center, g[f'{name}_{kind}_center'])
+            np.testing.assert_array_equal(b.rotation, g[f'{name}_{kind}_rotation'])
+            np.testing.assert_array_equal(b.axes, g[f'{name}_{kind}_axes'])
+            for m, seed in [(6, 11), (9, 190003)]:
+                u = O.sobol_points(5 if kind == 'box' else 4, m, seed)
+                r = O.compact_source(kind, b.center, b.rotation, b.axes, u)
+                key = f'{name}_{kind}_{m}_{seed}'
+                for f in ('origins', 'directions', 'weights'):
+                    np.testing.assert_array_equal(r[f], g[key + '_' + f], err_msg=key + f)
