@@ -451,6 +451,9 @@ constexpr int kMaxCaps = 96;
 constexpr int kFrontier = 64;
 constexpr int kLeafList = 64;
 constexpr int kMaxOpen = 8;
+constexpr int kRefRows = 24 + 48;      // rows of the refinement lattices (K = 24, 48)
+constexpr int kMaskWords = 128;        // > (samples of lattice 48) / 32
+constexpr int kCandList = 256;         // distinct candidate samples of one refinement level
 constexpr float kPi = 3.14159265358979f;
 
 struct ExposureWarp {
@@ -459,6 +462,8 @@ struct ExposureWarp {
     int front[2][kFrontier];
     int leaves[kLeafList];
     int open[2][kMaxOpen];             // open samples (row << 16 | index) of the last two levels
+    unsigned mask[kMaskWords];         // candidate samples of the current refinement level
+    int cand[kCandList];
     int n_front[2];
     int n_leaves, n_caps, whole;
 };
@@ -500,8 +505,28 @@ __global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* des
     __shared__ float4 dirs0[kLattice0Max];      // lattice 12: (x, y, z, id bits)
     __shared__ int row_start0[kLattice0 + 1];
     __shared__ ExposureWarp wsm[kExposureWarps];
+    __shared__ int rstart[kRefRows + kRefineLevels];    // per level: K + 1 row starts
+    __shared__ float2 rsc[kRefRows];                    // per level and row: (sin, cos) of theta
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu, below = (1u << lane) - 1u;
+    static_assert(kRefineLevels == 2, "refinement tables are sized for K = 24 and 48");
+    if (threadIdx.x == 32) {
+        for (int lv = 1; lv <= kRefineLevels; ++lv) {
+            const int K = kLattice0 << lv, r0 = kLattice0 * ((1 << lv) - 2), s0 = r0 + lv - 1;
+            int t = 0;
+            for (int k = 0; k < K; ++k) {
+                rstart[s0 + k] = t;
+                t += lattice_row_len(K, (k + 0.5f) * kPi / K);
+            }
+            rstart[s0 + K] = t;
+        }
+    }
+    for (int t = threadIdx.x; t < kRefRows; t += blockDim.x) {
+        const int lv = t < 24 ? 1 : 2, K = kLattice0 << lv, k = t - kLattice0 * ((1 << lv) - 2);
+        float sn, cs;
+        sincosf((k + 0.5f) * kPi / K, &sn, &cs);
+        rsc[t] = make_float2(sn, cs);
+    }
     if (threadIdx.x == 0) {
         int t = 0;
         for (int k = 0; k < kLattice0; ++k) {
@@ -603,32 +628,6 @@ __global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* des
         __syncwarp();
         const int nc = min(W.n_caps, kMaxCaps);
         bool buried = W.whole != 0;
-        // largest caps first (rank sort on cos alpha, ties by slot)
-        if (!buried && nc > 1) {
-            float4 mc[3];
-            float2 md[3];
-            int rk[3];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                const int i = lane + 32 * q;
-                rk[q] = -1;
-                if (i < nc) {
-                    mc[q] = W.cap[i];
-                    md[q] = W.dr[i];
-                    int r = 0;
-                    for (int o = 0; o < nc; ++o) {
-                        const float w = W.cap[o].w;
-                        r += (w < mc[q].w || (w == mc[q].w && o < i)) ? 1 : 0;
-                    }
-                    rk[q] = r;
-                }
-            }
-            __syncwarp();
-#pragma unroll
-            for (int q = 0; q < 3; ++q)
-                if (rk[q] >= 0) { W.cap[rk[q]] = mc[q]; W.dr[rk[q]] = md[q]; }
-            __syncwarp();
-        }
         bool exposed = nc == 0 && !buried;
         // 3a. lattice 12, every sample; open samples recorded
         int n_open = 0;
@@ -652,15 +651,20 @@ __global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* des
             __syncwarp();
             if (!buried && !exposed && n_open == 0) buried = true;
         }
-        // 3b. finer lattices around the open samples
+        // 3b. finer lattices around the open samples: mark the distinct candidates of
+        //     every open sample in a bit mask, then test them once each
         int side = 0;
         for (int lv = 1; lv <= kRefineLevels && !buried && !exposed; ++lv) {
             const int K = kLattice0 << lv, Kp = K >> 1;
+            const int r0 = kLattice0 * ((1 << lv) - 2);          // first row of this level in rsc
+            const int* rs = rstart + r0 + lv - 1;                // its K + 1 row starts
+            const int n_k = rs[K], words = (n_k + 31) >> 5;
             const float alpha = 1.05f * 3.f * kPi / K;            // 3 pi / K, widened
             const float ca = cosf(alpha);
             if (set_caps(W, nc, b.w, b.w * kPi / K, mS, lane)) { buried = true; break; }
-            int n_next = 0;
-            for (int u = 0; u < n_open && !exposed; ++u) {
+            for (int w = lane; w < words; w += 32) W.mask[w] = 0u;
+            __syncwarp();
+            for (int u = 0; u < n_open; ++u) {
                 const int idU = W.open[side][u];
                 const int kU = idU >> 16, lU = idU & 0xffff;
                 const float thU = (kU + 0.5f) * kPi / Kp;
@@ -669,70 +673,79 @@ __global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* des
                 sincosf(thU, &sU, &cU);
                 const int kmin = max(0, (int)ceilf((thU - alpha) * K / kPi - 0.5f) - 1);
                 const int kmax = min(K - 1, (int)floorf((thU + alpha) * K / kPi - 0.5f) + 1);
-                const int nrows = kmax - kmin + 1;                 // <= 9
-                // row q on lane q: samples l0 .. l0 + cnt - 1 (mod L) lie within alpha of U
-                int rk = 0, rL = 1, rl0 = 0, rcnt = 0;
-                float rs = 0.f, rc = 1.f;
-                if (lane < nrows) {
-                    rk = kmin + lane;
-                    const float th = (rk + 0.5f) * kPi / K;
-                    sincosf(th, &rs, &rc);
-                    rL = lattice_row_len(K, th);
-                    const float den = sU * rs;
-                    const float rhs = den > 1e-6f ? (ca - cU * rc) / den : -2.f;
-                    if (rhs <= -1.f) { rl0 = 0; rcnt = rL; }
+                if (lane <= kmax - kmin) {                         // row kmin + lane: samples within alpha of U
+                    const int rk = kmin + lane;
+                    const float2 sc = rsc[r0 + rk];
+                    const int rL = rs[rk + 1] - rs[rk];
+                    const float den = sU * sc.x;
+                    const float rhs = den > 1e-6f ? (ca - cU * sc.y) / den : -2.f;
+                    int l0 = 0, cnt = 0;
+                    if (rhs <= -1.f) { cnt = rL; }
                     else if (rhs <= 1.f) {
                         const float dphi = acosf(rhs) + 2.f * kPi / rL;
                         const int a0 = (int)ceilf((phU - dphi) * rL / (2.f * kPi));
                         const int a1 = (int)floorf((phU + dphi) * rL / (2.f * kPi));
-                        rcnt = a1 - a0 + 1;
-                        if (rcnt >= rL) { rl0 = 0; rcnt = rL; }
-                        else { rl0 = a0; rcnt = max(rcnt, 0); }
+                        cnt = a1 - a0 + 1;
+                        if (cnt >= rL) cnt = rL; else { l0 = a0; cnt = max(cnt, 0); }
+                    }
+                    for (int c = 0; c < cnt; ++c) {
+                        int l = (l0 + c) % rL;
+                        if (l < 0) l += rL;
+                        const int idx = rs[rk] + l;
+                        atomicOr(&W.mask[idx >> 5], 1u << (idx & 31));
                     }
                 }
-                int incl = rcnt;                                   // inclusive scan over the rows
+                __syncwarp();
+            }
+            // compact the marked samples into W.cand, in index order
+            int total = 0;
+            for (int wb = 0; wb < words; wb += 32) {
+                const int w = wb + lane;
+                unsigned bits = w < words ? W.mask[w] : 0u;
+                const int c = __popc(bits);
+                int incl = c;
 #pragma unroll
-                for (int o = 1; o < 16; o <<= 1) {
+                for (int o = 1; o < 32; o <<= 1) {
                     const int v = __shfl_up_sync(full, incl, o);
                     if (lane >= o) incl += v;
                 }
-                const int total = __shfl_sync(full, incl, nrows - 1);
-                for (int base = 0; base < total && !exposed; base += 32) {
-                    const int t = base + lane;
-                    bool miss = false;
-                    int id = 0;
-                    // row of candidate t: first q with incl[q] > t
-                    int q_sel = -1, excl = 0;
-                    for (int q = 0; q < nrows; ++q) {
-                        const int iq = __shfl_sync(full, incl, q);
-                        const int cq = __shfl_sync(full, rcnt, q);
-                        if (q_sel < 0 && t < iq) { q_sel = q; excl = iq - cq; }
-                    }
-                    const int qk = __shfl_sync(full, rk, q_sel < 0 ? 0 : q_sel);
-                    const int qL = __shfl_sync(full, rL, q_sel < 0 ? 0 : q_sel);
-                    const int ql0 = __shfl_sync(full, rl0, q_sel < 0 ? 0 : q_sel);
-                    const float qs = __shfl_sync(full, rs, q_sel < 0 ? 0 : q_sel);
-                    const float qc = __shfl_sync(full, rc, q_sel < 0 ? 0 : q_sel);
-                    if (t < total && q_sel >= 0) {
-                        int l = (ql0 + (t - excl)) % qL;
-                        if (l < 0) l += qL;
-                        float sp, cp;
-                        sincosf(2.f * kPi * (float)l / (float)qL, &sp, &cp);
-                        miss = !in_some_cap(W, nc, qs * cp, qs * sp, qc);
-                        id = (qk << 16) | l;
-                        if (miss)
-                            for (int o = 0; o < n_next && o < kMaxOpen; ++o)
-                                if (W.open[side ^ 1][o] == id) { miss = false; break; }   // already open
-                    }
-                    const unsigned m = __ballot_sync(full, miss);
-                    const int at = n_next + __popc(m & below);
-                    __syncwarp();
-                    if (miss && at < kMaxOpen) W.open[side ^ 1][at] = id;
-                    n_next += __popc(m);
-                    exposed = n_next > kMaxOpen;
-                    __syncwarp();
+                int at = total + incl - c;
+                while (bits) {
+                    const int bit = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    if (at < kCandList) W.cand[at] = (w << 5) + bit;
+                    ++at;
                 }
+                total += __shfl_sync(full, incl, 31);
             }
+            __syncwarp();
+            if (total > kCandList) { exposed = true; break; }   // too many to test: keep the atom
+            int n_next = 0;
+            for (int base = 0; base < total && !exposed; base += 32) {
+                const int t = base + lane;
+                bool miss = false;
+                int id = 0;
+                if (t < total) {
+                    const int idx = W.cand[t];
+                    int lo_k = 0, hi_k = K - 1;                      // row: last k with rs[k] <= idx
+                    while (lo_k < hi_k) {
+                        const int mid = (lo_k + hi_k + 1) >> 1;
+                        if (rs[mid] <= idx) lo_k = mid; else hi_k = mid - 1;
+                    }
+                    const int l = idx - rs[lo_k], L = rs[lo_k + 1] - rs[lo_k];
+                    const float2 sc = rsc[r0 + lo_k];
+                    float sp, cp;                                    // phi - pi keeps the fast sincos in range
+                    __sincosf(2.f * kPi * (float)l / (float)L - kPi, &sp, &cp);
+                    miss = !in_some_cap(W, nc, -sc.x * cp, -sc.x * sp, sc.y);
+                    id = (lo_k << 16) | l;
+                }
+                const unsigned m = __ballot_sync(full, miss);
+                const int at = n_next + __popc(m & below);
+                if (miss && at < kMaxOpen) W.open[side ^ 1][at] = id;
+                n_next += __popc(m);
+                exposed = n_next > kMaxOpen;
+            }
+            __syncwarp();
             if (exposed) break;
             if (n_next == 0) buried = true;
             else if (lv == kRefineLevels) exposed = true;
