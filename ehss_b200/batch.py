@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import ctypes as ct
 import math
+from collections.abc import Sequence
 
 import numpy as np
 
@@ -136,6 +137,7 @@ class BatchCCS:
             for k, seed in enumerate(seed_schedule(sd, repeats)):
                 jobs.append(BlockJob(sc, lg, seed, cap=cap, precision=prec, ehss=ehss, pa=pa, tag=(s, k)))
         self.repeats = int(repeats)
+        self.ehss, self.pa = bool(ehss), bool(pa)
         self.cap_ladder = tuple(int(c) for c in cap_ladder) if cap_ladder else ()
         self.tail_fraction = float(tail_fraction)
         rays = sum(1 << j.log2_rays for j in jobs)
@@ -159,26 +161,37 @@ class BatchCCS:
         self.plan.run()
 
     def download(self):
-        blocks = self.plan.collect()
-        if self.cap_ladder:
-            blocks = self.plan.extend_caps(self.cap_ladder, self.tail_fraction, results=blocks)
+        """Per-structure summaries (one device-to-host copy).  Each structure's
+        ``runs`` lists its blocks' full read-outs, built on first access."""
         S, R = len(self.scenes), self.repeats
-        out = [dict(structure=s, atoms=sc.n_atoms, runs=blocks[s * R:(s + 1) * R]) for s, sc in enumerate(self.scenes)]
+        if self.cap_ladder:
+            blocks = self.plan.extend_caps(self.cap_ladder, self.tail_fraction)
+            ehss = np.array([b.get('ehss_angstrom2', 0.) for b in blocks])
+            tail = np.array([b.get('tail_bound_angstrom2', 0.) for b in blocks])
+            pa = np.array([b.get('pa_angstrom2', 0.) for b in blocks])
+            unres = np.array([b.get('unresolved_rays', 0) for b in blocks])
+            runs = [blocks[s * R:(s + 1) * R] for s in range(S)]
+        else:
+            packed = self.plan.fetch()
+            t = self.plan.totals(packed)
+            ehss, tail, pa, unres = t['ehss'], t['tail'], t['pa'], t['unresolved']
+            lazy = _BlockReadout(self.plan, packed)
+            runs = [_Runs(lazy, s * R, (s + 1) * R) for s in range(S)]
+        out = [dict(structure=s, atoms=sc.n_atoms, runs=runs[s]) for s, sc in enumerate(self.scenes)]
 
-        def summaries(key):
-            a = np.array([b[key] for b in blocks]).reshape(S, R)
+        def summaries(values):
+            a = np.asarray(values).reshape(S, R)
             mean = a.mean(axis=1).tolist()
             sd = a.std(axis=1, ddof=1).tolist() if R > 1 else [None] * S
             return [dict(mean=m, sd=d, sem=d / math.sqrt(R) if d is not None else None, replicates=R)
                     for m, d in zip(mean, sd)]
-        if 'ehss_angstrom2' in blocks[0]:
-            ehss = summaries('ehss_angstrom2')
-            tails = np.array([b['tail_bound_angstrom2'] for b in blocks]).reshape(S, R).mean(axis=1).tolist()
-            unres = np.array([b['unresolved_rays'] for b in blocks]).reshape(S, R).sum(axis=1).tolist()
-            for o, e, t, u in zip(out, ehss, tails, unres):
-                o.update(ehss_angstrom2=e, ehss_tail_bound_mean_angstrom2=t, ehss_unresolved_rays_total=int(u))
-        if 'pa_angstrom2' in blocks[0]:
-            for o, p in zip(out, summaries('pa_angstrom2')):
+        if self.ehss:
+            tails = np.asarray(tail).reshape(S, R).mean(axis=1).tolist()
+            unr = np.asarray(unres).reshape(S, R).sum(axis=1).tolist()
+            for o, e, tl, u in zip(out, summaries(ehss), tails, unr):
+                o.update(ehss_angstrom2=e, ehss_tail_bound_mean_angstrom2=tl, ehss_unresolved_rays_total=int(u))
+        if self.pa:
+            for o, p in zip(out, summaries(pa)):
                 o['pa_angstrom2'] = p
         return out
 
@@ -188,3 +201,34 @@ class BatchCCS:
         self.build()
         self.trace()
         return self.download()
+
+
+class _BlockReadout:
+    """Block dicts of one fetched result, built once when first needed."""
+
+    def __init__(self, plan, packed):
+        self.plan, self.packed, self.blocks = plan, packed, None
+
+    def get(self):
+        if self.blocks is None:
+            self.blocks = self.plan.readout(self.packed)
+        return self.blocks
+
+
+class _Runs(Sequence):
+    """One structure's blocks (a read-only list view, materialised lazily)."""
+
+    def __init__(self, readout, begin, end):
+        self._r, self._b, self._e = readout, begin, end
+
+    def __len__(self):
+        return self._e - self._b
+
+    def __getitem__(self, i):
+        return self._r.get()[self._b:self._e][i]
+
+    def __eq__(self, other):
+        return list(self) == list(other)
+
+    def __repr__(self):
+        return repr(list(self))

@@ -154,21 +154,37 @@ class BlockPlan:
         else:
             self.enqueue()
 
-    def collect(self):
-        """Copy results to the host; returns one dict per block (synchronises).
-
-        One device-to-host copy brings the block totals, histograms and
-        ledgers; the read-out is vectorised over blocks.
-        """
+    def fetch(self):
+        """One device-to-host copy of every block's totals, histogram and
+        ledger (synchronises); raises if a block reported a device failure."""
         packed = self.packed.cpu().numpy().view(np.uint64)
+        n = len(self.jobs)
+        res = packed[:n * _RESULT_WORDS].reshape(n, _RESULT_WORDS)
+        errors = res[:, _STATS0 + _lib.STAT_ERRORS]
+        if errors.any():
+            i = int(np.flatnonzero(errors)[0])
+            raise _lib.EHSSDeviceError(f'block {self.jobs[i].tag!r}: {int(errors[i])} bounded device failures')
+        return packed
+
+    def totals(self, packed):
+        """Per-block EHSS, tail bound and PA (float64 arrays, same arithmetic as
+        ``readout``) and unresolved counts from a ``fetch`` result."""
+        n = len(self.jobs)
+        res = packed[:n * _RESULT_WORDS].reshape(n, _RESULT_WORDS)
+        w = self._w
+        return dict(ehss=w * (res[:, 0].astype(np.float64) * _lib.FX_SCALE), tail=2 * w * res[:, 2].astype(np.float64),
+                    pa=w * res[:, 4].astype(np.float64), unresolved=res[:, 2].astype(np.int64))
+
+    def collect(self):
+        """Copy results to the host; returns one dict per block (synchronises)."""
+        return self.readout(self.fetch())
+
+    def readout(self, packed):
+        """One dict per block from a ``fetch`` result (vectorised over blocks)."""
         n = len(self.jobs)
         nw = n * _RESULT_WORDS
         res = packed[:nw].reshape(n, _RESULT_WORDS)
         stats = res[:, _STATS0:_STATS0 + _lib.NSTATS]
-        errors = stats[:, _lib.STAT_ERRORS]
-        if errors.any():
-            i = int(np.flatnonzero(errors)[0])
-            raise _lib.EHSSDeviceError(f'block {self.jobs[i].tag!r}: {int(errors[i])} bounded device failures')
         H = self.hist_len
         hist = packed[nw:nw + H].astype(np.int64).tolist()
         ledger = (packed[nw + H:nw + 2 * H].astype(np.float64) * _lib.FX_SCALE * self._w_entry).tolist()
