@@ -493,14 +493,21 @@ __device__ __forceinline__ bool set_caps(ExposureWarp& W, int nc, float r, float
 }
 
 __device__ __forceinline__ bool in_some_cap(const ExposureWarp& W, int nc, float sx, float sy, float sz) {
-    for (int c = 0; c < nc; ++c) {
+    int c = 0;
+    for (; c + 4 <= nc; c += 4) {          // four caps per step: their loads overlap
+        const float4 u0 = W.cap[c], u1 = W.cap[c + 1], u2 = W.cap[c + 2], u3 = W.cap[c + 3];
+        const bool h = (sx * u0.x + sy * u0.y + sz * u0.z >= u0.w) | (sx * u1.x + sy * u1.y + sz * u1.z >= u1.w) |
+                       (sx * u2.x + sy * u2.y + sz * u2.z >= u2.w) | (sx * u3.x + sy * u3.y + sz * u3.z >= u3.w);
+        if (h) return true;
+    }
+    for (; c < nc; ++c) {
         const float4 u = W.cap[c];
         if (sx * u.x + sy * u.y + sz * u.z >= u.w) return true;
     }
     return false;
 }
 
-__global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* descs, const int32_t* atom_scene,
+__global__ void __launch_bounds__(32 * kExposureWarps, 4) k_exposure(BuildDesc* descs, const int32_t* atom_scene,
                                                                   int64_t N, uint8_t* culled) {
     __shared__ float4 dirs0[kLattice0Max];      // lattice 12: (x, y, z, id bits)
     __shared__ int row_start0[kLattice0 + 1];
@@ -628,6 +635,35 @@ __global__ void __launch_bounds__(32 * kExposureWarps) k_exposure(BuildDesc* des
         __syncwarp();
         const int nc = min(W.n_caps, kMaxCaps);
         bool buried = W.whole != 0;
+        // caps wider than a hemisphere first: most samples then stop at the first few
+        if (!buried && nc > 32) {
+            float4 mc[3];
+            float2 md[3];
+            bool big[3];
+            int n_big = 0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const int i = lane + 32 * q;
+                big[q] = false;
+                if (i < nc) { mc[q] = W.cap[i]; md[q] = W.dr[i]; big[q] = mc[q].w < 0.f; }
+                n_big += __popc(__ballot_sync(full, big[q]));
+            }
+            __syncwarp();
+            int before_big = 0, before_small = 0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const int i = lane + 32 * q;
+                const unsigned mb = __ballot_sync(full, big[q]), ms = __ballot_sync(full, i < nc && !big[q]);
+                if (i < nc) {
+                    const int at = big[q] ? before_big + __popc(mb & below) : n_big + before_small + __popc(ms & below);
+                    W.cap[at] = mc[q];
+                    W.dr[at] = md[q];
+                }
+                before_big += __popc(mb);
+                before_small += __popc(ms);
+            }
+            __syncwarp();
+        }
         bool exposed = nc == 0 && !buried;
         // 3a. lattice 12, every sample; open samples recorded
         int n_open = 0;
