@@ -473,6 +473,7 @@ struct WarpAcc {
     unsigned hits, unresolved, escaped, pa;
     unsigned queries, grazing, fallback, fp64, errors, pad;
     unsigned long long box, sphere;
+    uint4 q0;
 };
 
 struct LaneRay {
@@ -664,7 +665,7 @@ __device__ __forceinline__ bool next_chunk(unsigned long long* counters, int n_p
 }
 
 template <bool EXACT, bool COUNT>
-__global__ void __launch_bounds__(128, 6) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
+__global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
                                                    int chunk_rays, int resolve_batch, ehss_block_result* results,
                                                    uint64_t* hist, uint64_t* ledger, unsigned long long* work,
                                                    int n_parts, int smem_stack, ehss_residual* residual,
@@ -703,6 +704,8 @@ __global__ void __launch_bounds__(128, 6) k_blocks(const ehss_block* blocks, int
         const int n_nodes = S.h->n_nodes;
         if (lane < kSmemBins) { A.count[lane] = 0; A.ledger[lane] = 0; }
         if (lane == 0) {
+            const uint4 b0 = make_uint4(B->base[0], B->base[1], B->base[2], B->base[3]);
+            A.q0 = block_point(reinterpret_cast<const uint4*>(B->basis), b0, (uint32_t)ray0);
             A.angle_fx = 0; A.hits = A.unresolved = A.escaped = A.pa = 0;
             A.queries = A.grazing = A.fallback = A.fp64 = 0;
             A.errors = ok ? 0 : 1;
@@ -775,8 +778,8 @@ __global__ void __launch_bounds__(128, 6) k_blocks(const ehss_block* blocks, int
                 if (status == kNeedRay) {
                     int p = pool + __popc(need & lt_mask);
                     if (p < cnt) {
-                        const uint4 base = make_uint4(B->base[0], B->base[1], B->base[2], B->base[3]);
-                        uint4 q = block_point(reinterpret_cast<const uint4*>(B->basis), base, (uint32_t)(ray0 + p));
+                        // ray0 is a multiple of the chunk size, so point(ray0 + p) = point(ray0) ^ B(p)
+                        uint4 q = block_point(reinterpret_cast<const uint4*>(B->basis), A.q0, (uint32_t)p);
                         Ray64 ray = impact_ray(q, S.h->center, S.h->radius);
 #pragma unroll
                         for (int i = 0; i < 3; ++i) { L.o[i] = ray.o[i]; L.d[i] = ray.d[i]; L.din[i] = ray.d[i]; }
