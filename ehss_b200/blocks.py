@@ -26,7 +26,7 @@ from .device import empty, ptr, stream_handle, torch
 
 _RESULT_WORDS = ct.sizeof(_lib.BlockResult) // 8
 _STATS0 = _lib.BlockResult.stats.offset // 8
-DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=8, chunk_rays=256, resolve_batch=24, smem_stack=8,
+DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=8, chunk_rays=256, resolve_batch=28, smem_stack=5,
                       count_tests=False)
 
 
