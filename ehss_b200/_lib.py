@@ -21,6 +21,8 @@ STAT_BOX, STAT_SPHERE, STAT_QUERIES, STAT_GRAZING, STAT_FALLBACK, STAT_FP64, STA
 NSTATS = 8
 BLOCK_EHSS, BLOCK_PA = 1, 2
 LAUNCH_COUNT_TESTS = 1
+# LBVH leaf bound used by default: leaves of 13-16 atoms trace fastest on B200 with the default launch
+DEFAULT_LEAF = 14
 BUILD_EXTERIOR = 1
 FX_SCALE = 2.0 ** -40
 

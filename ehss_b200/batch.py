@@ -49,7 +49,7 @@ class BatchScenes:
     block trace may use because all its rays start outside the union.
     """
 
-    def __init__(self, structures, leaf_size=8, device=None, exterior=False):
+    def __init__(self, structures, leaf_size=_lib.DEFAULT_LEAF, device=None, exterior=False):
         lib = _lib.load()
         t = torch()
         self.device = require_cuda(device)
@@ -122,7 +122,7 @@ class BatchScenes:
 
 class BatchCCS:
     def __init__(self, structures, log2_rays, seeds, repeats=3, cap=64, precision='fp32', ehss=True, pa=False,
-                 leaf_size=8, launch=None, device=None, graph=True, exterior=True, cap_ladder=None,
+                 leaf_size=_lib.DEFAULT_LEAF, launch=None, device=None, graph=True, exterior=True, cap_ladder=None,
                  tail_fraction=5e-4):
         S = len(structures)
         log2s = [int(log2_rays)] * S if np.isscalar(log2_rays) else [int(x) for x in log2_rays]

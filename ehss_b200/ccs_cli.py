@@ -222,7 +222,7 @@ def parser():
     p.add_argument('--repeats', type=int, default=3, help='Independent scrambled Sobol replicates (default: 3)')
     p.add_argument('--seed', type=int, default=190003)
     p.add_argument('--threads', type=int, default=1, help='Accepted for compatibility; the GPU replaces CPU threads')
-    p.add_argument('--leaf-size', type=int, default=8, help='Maximum atoms per device LBVH leaf (1..16, default: 8)')
+    p.add_argument('--leaf-size', type=int, default=14, help='Maximum atoms per device LBVH leaf (1..16, default: 14)')
     p.add_argument('--max-collisions', type=int, default=64)
     p.add_argument('--probe-radius', type=float, default=1.4, help='Added probe radius in angstrom (default: 1.4, He scenario)')
     p.add_argument('--radii-json', type=Path, help='Overrides/additions to atomic VDW radii in angstrom, never effective radii')

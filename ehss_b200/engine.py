@@ -51,7 +51,7 @@ class Scene:
     (ehss_static.py:68-69).
     """
 
-    def __init__(self, centers, radii, leaf_size=8, device=None, exterior=False):
+    def __init__(self, centers, radii, leaf_size=_lib.DEFAULT_LEAF, device=None, exterior=False):
         lib = _lib.load()
         self.device = require_cuda(device)
         c = np.ascontiguousarray(centers, dtype=np.float64)
@@ -87,7 +87,7 @@ class Scene:
         self.radius = float(info.radius)
 
     @classmethod
-    def from_spheres(cls, spheres, leaf_size=8, device=None):
+    def from_spheres(cls, spheres, leaf_size=_lib.DEFAULT_LEAF, device=None):
         return cls(spheres.centers, spheres.radii, leaf_size, device)
 
     def source_rays(self, power, seed, first=0, n=None):

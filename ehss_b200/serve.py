@@ -171,11 +171,12 @@ class CCSServer:
 class DeviceExecutor:
     """The device side of the server: batched scene builds and fused block rounds."""
 
-    def __init__(self, leaf_size=8, cap=64, precision='fp32', launch=None, device=None):
+    def __init__(self, leaf_size=None, cap=64, precision='fp32', launch=None, device=None):
         from . import _lib
         from .device import require_cuda
         self.device = require_cuda(device)
-        self.leaf_size, self.cap, self.launch = leaf_size, cap, launch
+        self.leaf_size = _lib.DEFAULT_LEAF if leaf_size is None else int(leaf_size)
+        self.cap, self.launch = cap, launch
         self.precision = {'fp64': _lib.PREC_FP64, 'fp32': _lib.PREC_FP32}[precision]
 
     def footprint(self, n_atoms):
