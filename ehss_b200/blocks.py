@@ -26,8 +26,22 @@ from .device import empty, ptr, stream_handle, torch
 
 _RESULT_WORDS = ct.sizeof(_lib.BlockResult) // 8
 _STATS0 = _lib.BlockResult.stats.offset // 8
-DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=8, chunk_rays=256, resolve_batch=28, smem_stack=5,
+# chunk_rays 0: sized to the work (auto_chunk)
+DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=8, chunk_rays=0, resolve_batch=28, smem_stack=5,
                       count_tests=False)
+
+
+def auto_chunk(rays, launch, sm_count):
+    """Rays per work item: 256 when every warp of the persistent grid gets
+    several chunks (large batches), smaller for small jobs so that a single
+    structure's blocks spread over all warps instead of queueing behind a
+    few long chunks (power of two in 32..256)."""
+    warps = sm_count * int(launch['ctas_per_sm']) * (int(launch['block_threads']) // 32)
+    target = max(1, int(rays) // (4 * warps))
+    chunk = 32
+    while chunk < 256 and chunk * 2 <= target:
+        chunk *= 2
+    return chunk
 
 
 @dataclass
@@ -59,6 +73,9 @@ class BlockPlan:
         self.device = jobs[0].scene.device if device is None else device
         L = dict(DEFAULT_LAUNCH)
         L.update(launch or {})
+        if not L['chunk_rays']:
+            sms = t.cuda.get_device_properties(self.device).multi_processor_count if t.cuda.is_available() else 148
+            L['chunk_rays'] = auto_chunk(sum(1 << j.log2_rays for j in self.jobs), L, sms)
         precisions = 0
         for j in jobs:
             precisions |= 1 << int(j.precision)
