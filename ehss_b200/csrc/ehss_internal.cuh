@@ -73,7 +73,7 @@ struct SceneView {
 
 __host__ __device__ inline uint64_t align256(uint64_t x) { return (x + 255u) & ~uint64_t(255); }
 
-inline void scene_layout(int64_t n, uint64_t* off_nodes, uint64_t* off_atoms, uint64_t* off_atoms64,
+__host__ __device__ inline void scene_layout(int64_t n, uint64_t* off_nodes, uint64_t* off_atoms, uint64_t* off_atoms64,
                          uint64_t* off_ids, uint64_t* off_rank, uint64_t* total) {
     int64_t nodes = n > 1 ? n - 1 : 1;
     uint64_t o = 256;

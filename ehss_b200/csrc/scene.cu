@@ -73,7 +73,13 @@ __global__ void k_stats(BuildDesc* descs, int n_scenes) {
     const int64_t n = D.n;
     __shared__ double center[3];
     __shared__ int bad;
-    if (threadIdx.x == 0) bad = 0;
+    // header: zeroed, then the layout offsets (the rest is filled below and by k_emit_nodes)
+    if (threadIdx.x < sizeof(SceneHeader) / 4) reinterpret_cast<uint32_t*>(H)[threadIdx.x] = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bad = 0;
+        scene_layout(n, &H->off_nodes, &H->off_atoms, &H->off_atoms64, &H->off_ids, &H->off_rank, &H->bytes);
+    }
     __syncthreads();
     // Sequential sum, one lane per coordinate: numpy's mean(axis=0) adds the
     // rows in order and divides by n (ehss_state.py:46).
@@ -896,19 +902,9 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
     W.cub_temp = p;
     W.cub_bytes = cub_sort_bytes(N);
 
-    // headers: layout offsets are host-computed, the rest is filled on device
-    for (int s = 0; s < S; ++s) {
-        SceneHeader h;
-        memset(&h, 0, sizeof(h));
-        uint64_t total;
-        scene_layout(n[s], &h.off_nodes, &h.off_atoms, &h.off_atoms64, &h.off_ids, &h.off_rank, &total);
-        h.bytes = total;
-        int rc = cuda_status(cudaMemcpyAsync(scenes[s], &h, sizeof(h), cudaMemcpyHostToDevice, stream),
-                             "scene header upload");
-        if (rc) { delete[] host; return rc; }
-    }
-    // A copy from pageable host memory has staged its source when the call
-    // returns, so the host descriptors (and the headers above) may go now.
+    // The headers are written on the device (k_stats); the descriptors are the
+    // only upload.  A copy from pageable host memory has staged its source
+    // when the call returns, so the host descriptors may go now.
     int rc = cuda_status(cudaMemcpyAsync(W.descs, host, sizeof(BuildDesc) * S, cudaMemcpyHostToDevice, stream),
                          "build descriptor upload");
     delete[] host;
