@@ -24,7 +24,7 @@ LAUNCH_COUNT_TESTS = 1
 # LBVH leaf bound used by default: leaves of 13-16 atoms trace fastest on B200 with the default launch
 DEFAULT_LEAF = 14
 BUILD_EXTERIOR = 1
-FX_SCALE = 2.0 ** -40
+FX_SCALE = 2.0 ** -36
 
 P = ct.c_void_p
 I32, I64, U64 = ct.c_int32, ct.c_int64, ct.c_uint64

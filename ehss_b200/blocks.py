@@ -10,7 +10,7 @@ launch in a CUDA graph so repeated runs cost one graph replay.
 
 Totals come back as integers (fixed point for angle sums), so every block's
 result is independent of what else shares the launch:
-    omega = w * angle_fx * 2^-40,  pa = w * hits,  tail = 2 * w * unresolved,
+    omega = w * angle_fx * 2^-36,  pa = w * hits,  tail = 2 * w * unresolved,
 with w = pi R^2 / 2**log2_rays.
 """
 from __future__ import annotations

@@ -272,7 +272,10 @@ int ehss_blocks_prepare(ehss_block* blocks, int n_blocks, const uint64_t* seeds,
     for (int b = 0; b < n_blocks; ++b) {
         ehss_block& B = blocks[b];
         if (!B.scene) { set_error("block %d: null scene", b); return EHSS_ERR_VALUE; }
-        if (B.log2_rays < 3 || B.log2_rays > 24) { set_error("block %d: log2_rays must be 3..24", b); return EHSS_ERR_VALUE; }
+        if (B.log2_rays < 3 || B.log2_rays > kMaxBlockLog2) {
+            set_error("block %d: log2_rays must be 3..%d", b, kMaxBlockLog2);
+            return EHSS_ERR_VALUE;
+        }
         if (B.cap < 1 || B.cap > 100000) { set_error("block %d: cap must be 1..100000", b); return EHSS_ERR_VALUE; }
         if (B.precision != EHSS_PREC_FP64 && B.precision != EHSS_PREC_FP32) { set_error("block %d: unknown precision", b); return EHSS_ERR_VALUE; }
         if (!(B.flags & (EHSS_BLOCK_EHSS | EHSS_BLOCK_PA))) { set_error("block %d: no work flags", b); return EHSS_ERR_VALUE; }

@@ -35,7 +35,11 @@ constexpr int kLeafBits = 4;                 // leaf reference: atom count - 1 i
 constexpr int kMaxLeaf = 1 << kLeafBits;
 constexpr int kEmptyChild = INT32_MIN;
 constexpr int kStackDepth = 96;   // >= 3 x the deepest 4-wide tree (binary LBVH height <= 55)
-constexpr int kMaxWorkParts = 512;    // per-SM work ranges of the persistent kernel (workspace 4 KiB)
+constexpr int kMaxWorkParts = 512;
+// Fixed point of the angle sums: a ray adds at most 2 * 2^36, so a block of up
+// to 2^26 rays sums below 2^63 (ehss_blocks_prepare enforces the bound).
+constexpr double kFxScale = 0x1p36;
+constexpr int kMaxBlockLog2 = 26;    // per-SM work ranges of the persistent kernel (workspace 4 KiB)
 
 struct alignas(256) SceneHeader {
     uint32_t magic;

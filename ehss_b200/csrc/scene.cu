@@ -86,7 +86,15 @@ __global__ void k_stats(BuildDesc* descs, int n_scenes) {
     if (threadIdx.x < 3) {
         int c = threadIdx.x;
         double acc = 0.;
-        for (int64_t i = 0; i < n; ++i) acc = dadd(acc, D.xyz[i * 3 + c]);
+        int64_t i = 0;
+        for (; i + 8 <= n; i += 8) {         // loads ahead of the (sequential) sum
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = D.xyz[(i + k) * 3 + c];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc = dadd(acc, v[k]);
+        }
+        for (; i < n; ++i) acc = dadd(acc, D.xyz[i * 3 + c]);
         center[c] = ddiv(acc, (double)n);
     }
     // validation and radii extrema

@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                     unsigned long long fx = 0;
                     if (escaped) {
                         double a = scatter_angle(L.din[0], L.din[1], L.din[2], L.d[0], L.d[1], L.d[2]);
-                        fx = __double2ull_rn(a * 0x1p40);
+                        fx = __double2ull_rn(a * kFxScale);
                         atomicAdd(&A.escaped, 1u);
                         if (fx) atomicAdd(&A.angle_fx, fx);
                     } else {
@@ -987,7 +987,7 @@ __global__ void __launch_bounds__(128) k_extend(const ehss_block* blocks, int nb
         atomicAdd((unsigned long long*)&h[count], 1ull);
         if (escaped) {
             const double ang = scatter_angle(R.din[0], R.din[1], R.din[2], d[0], d[1], d[2]);
-            const unsigned long long fx = __double2ull_rn(ang * 0x1p40);
+            const unsigned long long fx = __double2ull_rn(ang * kFxScale);
             atomicAdd((unsigned long long*)&E.escaped, 1ull);
             if (fx) {
                 atomicAdd((unsigned long long*)&E.angle_fx, fx);

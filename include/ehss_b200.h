@@ -222,10 +222,10 @@ int ehss_pa_grid(const void* scene_dev, int64_t n_atoms, int n_dirs, uint64_t se
  *
  * Sums are kept in integer fixed point so that every block's result is
  * independent of scheduling and of what else runs in the launch:
- *   omega     = w * angle_fx * 2^-40        (w = pi R^2 / 2^log2_rays)
+ *   omega     = w * angle_fx * 2^-36        (w = pi R^2 / 2^log2_rays)
  *   pa (same rays) = w * hits ;  tail bound = 2 * w * unresolved
  * hist/ledger rows have cap+1 entries (bincount of bounces, unweighted and
- * weighted by the contribution in 2^-40 units). */
+ * weighted by the contribution in 2^-36 units). */
 #define EHSS_BLOCK_EHSS 1u      /* trace EHSS */
 #define EHSS_BLOCK_PA 2u        /* any-hit PA on the same rays */
 
@@ -242,7 +242,7 @@ typedef struct ehss_block {
     uint32_t basis[30][4];    /* per position bit, [bit][dim] (offset 0) */
     uint32_t base[4];         /* offset 480 */
     const void* scene;        /* device scene buffer */
-    int32_t log2_rays;        /* 3..24 */
+    int32_t log2_rays;        /* 3..26 (the angle sum stays below 2^63) */
     int32_t cap;              /* collision cap >= 1 */
     int32_t precision;        /* EHSS_PREC_* */
     uint32_t flags;           /* EHSS_BLOCK_* */
@@ -252,7 +252,7 @@ typedef struct ehss_block {
 } ehss_block;
 
 typedef struct ehss_block_result {
-    uint64_t angle_fx;        /* sum of clip(1 - d_in.d_out, 0, 2) over escaped rays, 2^-40 units */
+    uint64_t angle_fx;        /* sum of clip(1 - d_in.d_out, 0, 2) over escaped rays, 2^-36 units */
     uint64_t hits;            /* rays with bounces > 0 or unresolved */
     uint64_t unresolved;
     uint64_t escaped;
@@ -312,7 +312,7 @@ typedef struct ehss_residual {
 } ehss_residual;
 
 typedef struct ehss_extension {   /* one row per extended block */
-    uint64_t angle_fx;    /* angle sum (2^-40 units) of the continued rays that escaped */
+    uint64_t angle_fx;    /* angle sum (2^-36 units) of the continued rays that escaped */
     uint64_t escaped;     /* continued rays that escaped */
     uint64_t unresolved;  /* continued rays still unresolved at the new cap */
     uint64_t continued;   /* continued rays */

@@ -82,6 +82,14 @@ def test_blocks_prepare_chunks_and_offsets(lib):
     assert lib.ehss_blocks_prepare(blocks, n, seeds, 256, ct.byref(total)) == 0
     assert total.value == 16 + 1 + 64
     assert [b.chunk_begin for b in blocks] == [0, 16, 17]
+    # the fixed-point angle sum of a block must stay below 2^63: at most 2^26 rays
+    one = (_lib.Block * 1)()
+    one[0].scene, one[0].cap, one[0].precision, one[0].flags, one[0].hist_offset = 0x1000, 8, 1, _lib.BLOCK_EHSS, -1
+    one[0].log2_rays = 27
+    assert lib.ehss_blocks_prepare(one, 1, (ct.c_uint64 * 1)(5), 256, ct.byref(total)) == _lib.ERR_VALUE
+    one[0].log2_rays = 26
+    assert lib.ehss_blocks_prepare(one, 1, (ct.c_uint64 * 1)(5), 256, ct.byref(total)) == 0
+    assert total.value == (1 << 26) // 256
     assert [b.hist_offset for b in blocks] == [0, 65, 67]
     blocks[1].cap = 0
     assert lib.ehss_blocks_prepare(blocks, n, seeds, 256, ct.byref(total)) == _lib.ERR_VALUE
@@ -164,7 +172,7 @@ def test_coherent_enumeration_is_the_sobol_point_set(lib, m, seed):
 
 def test_block_readout_matches_per_block_formulas():
     """BlockPlan.collect's vectorised read-out against the per-block definitions
-    omega = w angle_fx 2^-40, pa = w hits, tail = 2 w unresolved (host only)."""
+    omega = w angle_fx 2^-36, pa = w hits, tail = 2 w unresolved (host only)."""
     import torch
     from ehss_b200 import _lib
     from ehss_b200.blocks import BlockJob, BlockPlan, _RESULT_WORDS, _STATS0
