@@ -177,20 +177,9 @@ def solve_frame(spheres, args, progress=True):
         readout_s = (time.perf_counter() - tick) / len(rows)
         query_s = e0.elapsed_time(e1) * 1e-3 / len(rows)
         for row, res in zip(rows, results):
-            row['impact_source_s'] = 0.0            # generated inside the fused kernel
-            if bvh_pa:
-                row['pa'] = dict(pa_angstrom2=res['pa_angstrom2'], query_s=query_s, readout_s=readout_s,
-                                 box_tests=None, sphere_tests=None)
+            _frame_row(row, res, ehss, bvh_pa, query_s, readout_s)
             if ehss:
-                omega, tail = res['ehss_angstrom2'], res['tail_bound_angstrom2']
-                row['ehss'] = dict(ehss_angstrom2=omega, pa_from_same_rays_angstrom2=res['pa_from_same_rays_angstrom2'],
-                                   tail_bound_angstrom2=tail, sampled_interval_angstrom2=[omega, omega + tail],
-                                   unresolved_rays=res['unresolved_rays'], query_s=query_s,
-                                   collision_histogram=res['collision_histogram'],
-                                   collision_contribution_angstrom2=res['collision_contribution_angstrom2'],
-                                   box_tests=None, sphere_tests=None, readout_s=readout_s,
-                                   grazing_queries=res['grazing_queries'],
-                                   fp64_fallback_queries=res['fp64_fallback_queries'])
+                tail = res['tail_bound_angstrom2']
                 if progress:
                     print(f"  replicate {row['repeat']}/{args.repeats} (seed {row['seed']})", file=sys.stderr,
                           flush=True)
@@ -198,6 +187,29 @@ def solve_frame(spheres, args, progress=True):
                         print(f"  WARNING: {res['unresolved_rays']} unresolved rays; omitted contribution <= {tail:.6g} "
                               "A^2. Increase --max-collisions.", file=sys.stderr)
     total = time.perf_counter() - start
+    summary = _summary(rows, ehss, pa)
+    return dict(summary=summary, runs=rows,
+                timings=dict(ehss_setup_s=setup_s if ehss else 0., pa_setup_s=setup_s if bvh_pa else 0.,
+                             all_replicates_with_setup_s=total))
+
+
+def _frame_row(row, res, ehss, bvh_pa, query_s, readout_s):
+    row['impact_source_s'] = 0.0            # generated inside the fused kernel
+    if bvh_pa:
+        row['pa'] = dict(pa_angstrom2=res['pa_angstrom2'], query_s=query_s, readout_s=readout_s,
+                         box_tests=None, sphere_tests=None)
+    if ehss:
+        omega, tail = res['ehss_angstrom2'], res['tail_bound_angstrom2']
+        row['ehss'] = dict(ehss_angstrom2=omega, pa_from_same_rays_angstrom2=res['pa_from_same_rays_angstrom2'],
+                           tail_bound_angstrom2=tail, sampled_interval_angstrom2=[omega, omega + tail],
+                           unresolved_rays=res['unresolved_rays'], query_s=query_s,
+                           collision_histogram=res['collision_histogram'],
+                           collision_contribution_angstrom2=res['collision_contribution_angstrom2'],
+                           box_tests=None, sphere_tests=None, readout_s=readout_s,
+                           grazing_queries=res['grazing_queries'], fp64_fallback_queries=res['fp64_fallback_queries'])
+
+
+def _summary(rows, ehss, pa):
     summary = {}
     if pa:
         summary['pa_angstrom2'] = summarize([r['pa']['pa_angstrom2'] for r in rows])
@@ -205,9 +217,68 @@ def solve_frame(spheres, args, progress=True):
         summary['ehss_angstrom2'] = summarize([r['ehss']['ehss_angstrom2'] for r in rows])
         summary['ehss_tail_bound_mean_angstrom2'] = float(np.mean([r['ehss']['tail_bound_angstrom2'] for r in rows]))
         summary['ehss_unresolved_rays_total'] = sum(r['ehss']['unresolved_rays'] for r in rows)
-    return dict(summary=summary, runs=rows,
-                timings=dict(ehss_setup_s=setup_s if ehss else 0., pa_setup_s=setup_s if bvh_pa else 0.,
-                             all_replicates_with_setup_s=total))
+    return summary
+
+
+# frames traced together in one batched build and one persistent launch
+FRAME_BATCH_ATOMS = 2_000_000
+FRAME_BATCH_FRAMES = 1024
+
+
+def solve_frames(frames, args, progress=True):
+    """Many frames (``--all-frames``, several files) at once: one batched
+    scene build and one persistent launch for all replicates of a group of
+    frames, instead of one of each per frame.  Each frame's results are the
+    same integers as solve_frame's (block sums do not depend on what shares
+    the launch); timings are the group's, divided evenly over its frames."""
+    import torch
+    from .batch import BatchCCS
+    from .blocks import seed_schedule
+    ehss = args.method in ("ehss", "both")
+    pa = args.method in ("pa", "both")
+    bvh_pa = pa and args.pa_method == "bvh"
+    if not (ehss or bvh_pa):
+        return [solve_frame(s, args, progress) for s in frames]
+    out = []
+    i = 0
+    while i < len(frames):
+        group, atoms = [], 0
+        while i < len(frames) and len(group) < FRAME_BATCH_FRAMES and \
+                (not group or atoms + len(frames[i].radii) <= FRAME_BATCH_ATOMS):
+            group.append(frames[i]); atoms += len(frames[i].radii); i += 1
+        start = time.perf_counter()
+        seeds = seed_schedule(args.seed, args.repeats)
+        log2 = args.rays.bit_length() - 1
+        bc = BatchCCS([(s.centers, s.radii) for s in group], log2, [args.seed] * len(group), repeats=args.repeats,
+                      cap=args.max_collisions, precision='fp32', ehss=ehss, pa=bvh_pa,
+                      leaf_size=min(int(args.leaf_size), 16), graph=False)
+        bc.upload()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        bc.build()
+        e1.record()
+        bc.trace()
+        e2.record()
+        tick = time.perf_counter()
+        per = bc.download()
+        readout_s = (time.perf_counter() - tick) / (len(group) * args.repeats)
+        setup_s = e0.elapsed_time(e1) * 1e-3 / len(group)
+        query_s = e1.elapsed_time(e2) * 1e-3 / (len(group) * args.repeats)
+        total = (time.perf_counter() - start) / len(group)
+        for spheres, p in zip(group, per):
+            rows = [dict(repeat=k + 1, seed=sd) for k, sd in enumerate(seeds)]
+            if pa and args.pa_method == "adaptive":
+                from .adaptive_pa import adaptive_pa
+                for row in rows:
+                    row['pa'] = adaptive_pa(spheres, args.directions, args.grid_size, row['seed'])
+            for row, res in zip(rows, p['runs']):
+                _frame_row(row, res, ehss, bvh_pa, query_s, readout_s)
+            out.append(dict(summary=_summary(rows, ehss, pa), runs=rows,
+                            timings=dict(ehss_setup_s=setup_s if ehss else 0., pa_setup_s=setup_s if bvh_pa else 0.,
+                                         all_replicates_with_setup_s=total, batched_frames=len(group))))
+        if progress:
+            print(f"  traced {len(group)} frame(s) in one batch", file=sys.stderr, flush=True)
+    return out
 
 
 def parser():
@@ -297,10 +368,11 @@ def execute(args):
     solve_frame(Spheres(np.array([[0., 0., 0.], [2., 0., 0.]]), np.array([1., 1.])), warm, progress=False)
     warmup_s = time.perf_counter() - tick
     records = []
-    for spheres, info in jobs:
+    solved = solve_frames([s for s, _ in jobs], args) if len(jobs) > 1 else [None]
+    for (spheres, info), result in zip(jobs, solved):
         print(f"{Path(info['input_file']).name}, frame {info['frame']}, {info['selected_atoms']} atoms", file=sys.stderr,
               flush=True)
-        record = dict(**info, **solve_frame(spheres, args))
+        record = dict(**info, **(result if result is not None else solve_frame(spheres, args)))
         records.append(record)
         for name in ['pa_angstrom2', 'ehss_angstrom2']:
             if name in record['summary']:

@@ -363,3 +363,33 @@ def test_cli_end_to_end(eb, tmp_path):
     with pytest.raises(SystemExit) as e:
         ccs_cli.main([str(xyz), '--rays', '1000', '--output', str(tmp_path / 'bad')])
     assert e.value.code == 2
+
+
+def test_cli_all_frames_batched_equals_per_frame(eb, tmp_path):
+    """--all-frames traces every frame in one batched build and launch; each
+    frame's results equal solve_frame's for that frame alone."""
+    import json
+    from ehss_b200 import ccs_cli, workloads as W
+    c, _, el = W.globule(120, 3)
+    rng = np.random.default_rng(8)
+    frames = [c + rng.normal(scale=0.3, size=c.shape) for _ in range(5)]
+    lines = []
+    for k, f in enumerate(frames):
+        lines += [str(len(f)), f'frame {k}'] + [f'{e} {x:.6f} {y:.6f} {z:.6f}' for e, (x, y, z) in zip(el, f)]
+    xyz = tmp_path / 'traj.xyz'
+    xyz.write_text('\n'.join(lines) + '\n')
+    argv = ['--rays', '2048', '--repeats', '2', '--method', 'both', '--pa-method', 'bvh', '--max-collisions', '8']
+    assert ccs_cli.main([str(xyz), '--all-frames', '--output', str(tmp_path / 'all')] + argv) == 0
+    recs = json.loads((tmp_path / 'all' / 'results.json').read_text())['records']
+    assert len(recs) == 5 and all(r['timings']['batched_frames'] == 5 for r in recs)
+    table = ccs_cli.radius_table(None)
+    for k, rec in enumerate(recs):
+        frame = ccs_cli.read_xyz(xyz)[k]
+        spheres, _ = ccs_cli.prepare_frame(frame, table, 1.4)
+        args = ccs_cli.parser().parse_args([str(xyz), '--output', str(tmp_path / f'one{k}')] + argv)
+        one = ccs_cli.solve_frame(spheres, args, progress=False)
+        assert rec['summary']['ehss_angstrom2'] == one['summary']['ehss_angstrom2']
+        assert rec['summary']['pa_angstrom2'] == one['summary']['pa_angstrom2']
+        for a, b in zip(rec['runs'], one['runs']):
+            assert a['ehss']['collision_histogram'] == b['ehss']['collision_histogram']
+            assert a['ehss']['collision_contribution_angstrom2'] == b['ehss']['collision_contribution_angstrom2']
