@@ -359,10 +359,10 @@ def main():
     mean_trace_ms = float(np.mean(trace_ms))
     stats = np.sum([r['stats'] for r in bc.plan.collect()], axis=0)
     # one instrumented launch (outside the timed region): our own box/sphere tests per query
-    bc.plan.launch.options = _lib.LAUNCH_COUNT_TESTS
+    bc.plan.launch.options |= _lib.LAUNCH_COUNT_TESTS
     bc.plan.enqueue()
     cstats = np.sum([r['stats'] for r in bc.plan.collect()], axis=0)
-    bc.plan.launch.options = 0
+    bc.plan.launch.options &= ~_lib.LAUNCH_COUNT_TESTS
     own = {"box_tests_per_query": float(cstats[_lib.STAT_BOX]) / max(1, cstats[_lib.STAT_QUERIES]),
            "sphere_tests_per_query": float(cstats[_lib.STAT_SPHERE]) / max(1, cstats[_lib.STAT_QUERIES]),
            "queries_per_ray": float(cstats[_lib.STAT_QUERIES]) / rays_step}

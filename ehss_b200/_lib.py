@@ -21,9 +21,12 @@ STAT_BOX, STAT_SPHERE, STAT_QUERIES, STAT_GRAZING, STAT_FALLBACK, STAT_FP64, STA
 NSTATS = 8
 BLOCK_EHSS, BLOCK_PA = 1, 2
 LAUNCH_COUNT_TESTS = 1
+LAUNCH_RAY_BLOCKS = 2
+LAUNCH_NO_DISK_BLOCKS = 4
 # LBVH leaf bound used by default: leaves of 13-16 atoms trace fastest on B200 with the default launch
 DEFAULT_LEAF = 14
 BUILD_EXTERIOR = 1
+BLOCK_RAYS = 4
 FX_SCALE = 2.0 ** -36
 
 P = ct.c_void_p
@@ -39,12 +42,12 @@ class SceneInfo(ct.Structure):
 class Block(ct.Structure):
     _fields_ = [('basis', (ct.c_uint32 * 4) * 30), ('base', ct.c_uint32 * 4), ('scene', P), ('log2_rays', I32),
                 ('cap', I32), ('precision', I32), ('flags', ct.c_uint32), ('hist_offset', I64),
-                ('chunk_begin', I64), ('reserved', I64)]
+                ('chunk_begin', I64), ('rays', P), ('ray_scale', ct.c_double), ('reserved', I64)]
 
 
 class BlockResult(ct.Structure):
     _fields_ = [('angle_fx', U64), ('hits', U64), ('unresolved', U64), ('escaped', U64), ('pa_blocked', U64),
-                ('stats', U64 * NSTATS)]
+                ('hits_fx', U64), ('unresolved_fx', U64), ('pa_fx', U64), ('stats', U64 * NSTATS)]
 
 
 class Residual(ct.Structure):

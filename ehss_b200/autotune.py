@@ -11,6 +11,7 @@ $XDG_CACHE_HOME/ehss_b200/autotune.json (default ~/.cache).
 """
 from __future__ import annotations
 
+import dataclasses
 import json
 import os
 from pathlib import Path
@@ -46,7 +47,7 @@ def to_launch(cfg):
 
 def time_config(jobs, cfg, repeats=2):
     t = torch()
-    plan = BlockPlan([BlockJob(j.scene, j.log2_rays, j.seed, j.cap, j.precision, j.ehss, j.pa, j.tag) for j in jobs],
+    plan = BlockPlan([dataclasses.replace(j) for j in jobs],
                      launch=to_launch(cfg))
     plan.enqueue()
     best = float('inf')

@@ -123,7 +123,7 @@ class BatchScenes:
 class BatchCCS:
     def __init__(self, structures, log2_rays, seeds, repeats=3, cap=64, precision='fp32', ehss=True, pa=False,
                  leaf_size=_lib.DEFAULT_LEAF, launch=None, device=None, graph=True, exterior=True, cap_ladder=None,
-                 tail_fraction=5e-4):
+                 tail_fraction=5e-4, boundary=None):
         S = len(structures)
         log2s = [int(log2_rays)] * S if np.isscalar(log2_rays) else [int(x) for x in log2_rays]
         seeds = [int(x) for x in (seeds if not np.isscalar(seeds) else [seeds] * S)]
@@ -132,10 +132,21 @@ class BatchCCS:
         self.scenes = self.batch.scenes
         self.n_atoms = self.batch.n_atoms
         prec = {'fp64': _lib.PREC_FP64, 'fp32': _lib.PREC_FP32}[precision] if isinstance(precision, str) else precision
+        if boundary is not None and cap_ladder:
+            raise ValueError('cap extension needs impact-disk blocks; choose boundary=None or no cap_ladder')
+        fits = [None] * S
+        if boundary is not None:
+            # incidence on an enclosing boundary of each structure (CompactBoundary.fit, on the host)
+            from types import SimpleNamespace
+            from .compact import CompactBoundary
+            fits = [CompactBoundary.fit(SimpleNamespace(centers=np.asarray(c, dtype=np.float64),
+                                                        radii=np.asarray(r, dtype=np.float64)), boundary,
+                                        device=self.device) for c, r in structures]
         jobs = []
         for s, (sc, lg, sd) in enumerate(zip(self.scenes, log2s, seeds)):
             for k, seed in enumerate(seed_schedule(sd, repeats)):
-                jobs.append(BlockJob(sc, lg, seed, cap=cap, precision=prec, ehss=ehss, pa=pa, tag=(s, k)))
+                jobs.append(BlockJob(sc, lg, seed, cap=cap, precision=prec, ehss=ehss, pa=pa, tag=(s, k),
+                                     boundary=fits[s]))
         self.repeats = int(repeats)
         self.ehss, self.pa = bool(ehss), bool(pa)
         self.cap_ladder = tuple(int(c) for c in cap_ladder) if cap_ladder else ()

@@ -54,6 +54,7 @@ class BlockJob:
     ehss: bool = True
     pa: bool = False
     tag: object = None
+    boundary: object = None       # compact.CompactBoundary: its rays and weights instead of the impact disk
 
 
 class BlockPlan:
@@ -79,10 +80,14 @@ class BlockPlan:
         precisions = 0
         for j in jobs:
             precisions |= 1 << int(j.precision)
+        options = _lib.LAUNCH_COUNT_TESTS if L['count_tests'] else 0
+        n_boundary = sum(j.boundary is not None for j in jobs)
+        if n_boundary:
+            options |= _lib.LAUNCH_RAY_BLOCKS | (_lib.LAUNCH_NO_DISK_BLOCKS if n_boundary == len(jobs) else 0)
         self.launch = _lib.Launch(int(L['block_threads']), int(L['ctas_per_sm']), int(L['chunk_rays']),
-                                  int(L['resolve_batch']), precisions,
-                                  _lib.LAUNCH_COUNT_TESTS if L['count_tests'] else 0, int(L['smem_stack']), 0)
+                                  int(L['resolve_batch']), precisions, options, int(L['smem_stack']), 0)
         n = len(self.jobs)
+        self._ray_buffers = []
         host = (_lib.Block * n)()
         seeds = (ct.c_uint64 * n)()
         offset = 0
@@ -95,6 +100,18 @@ class BlockPlan:
             b.cap = int(j.cap)
             b.precision = int(j.precision)
             b.flags = (_lib.BLOCK_EHSS if j.ehss else 0) | (_lib.BLOCK_PA if j.pa else 0)
+            if j.boundary is not None:
+                # rays of an enclosing boundary, generated once on the device; weights are
+                # summed relative to the largest possible one (ray_scale)
+                if residual_capacity:
+                    raise ValueError('cap extension needs impact-disk blocks; boundary blocks keep their cap')
+                nr = 1 << int(j.log2_rays)
+                buf = t.empty(7 * nr, dtype=t.float64, device=self.device)
+                j.boundary.fill_ray_buffer(int(j.log2_rays), int(j.seed), buf)
+                self._ray_buffers.append(buf)
+                b.flags |= _lib.BLOCK_RAYS
+                b.rays = buf.data_ptr()
+                b.ray_scale = nr / j.boundary.max_projected_area()
             b.hist_offset = offset
             offset += j.cap + 1
             seeds[i] = int(j.seed)
@@ -112,7 +129,10 @@ class BlockPlan:
         self.hist_len = H
         self.d2h_bytes = self.packed.numel() * 8
         self._radius = [float(j.scene.radius) for j in self.jobs]
-        self._w = np.array([np.pi * R * R / (1 << j.log2_rays) for R, j in zip(self._radius, self.jobs)])
+        # weight per ray (impact disk) or the reference weight of a boundary block's weighted sums
+        self._w = np.array([1.0 / host[i].ray_scale if j.boundary is not None else np.pi * R * R / (1 << j.log2_rays)
+                            for i, (R, j) in enumerate(zip(self._radius, self.jobs))])
+        self._weighted = np.array([j.boundary is not None for j in self.jobs])
         self._offsets = [int(host[i].hist_offset) for i in range(n)]
         self._w_entry = np.zeros(H)
         for i, j in enumerate(self.jobs):
@@ -189,8 +209,20 @@ class BlockPlan:
         n = len(self.jobs)
         res = packed[:n * _RESULT_WORDS].reshape(n, _RESULT_WORDS)
         w = self._w
-        return dict(ehss=w * (res[:, 0].astype(np.float64) * _lib.FX_SCALE), tail=2 * w * res[:, 2].astype(np.float64),
-                    pa=w * res[:, 4].astype(np.float64), unresolved=res[:, 2].astype(np.int64))
+        _, unres_w, pa_w = self._weighted_counts(res)
+        return dict(ehss=w * (res[:, 0].astype(np.float64) * _lib.FX_SCALE), tail=2 * w * unres_w,
+                    pa=w * pa_w, unresolved=res[:, 2].astype(np.int64))
+
+    def _weighted_counts(self, res):
+        """Hits, unresolved and PA hits as float64: counts for impact-disk blocks,
+        weighted sums (in units of the reference weight) for boundary blocks."""
+        out = []
+        for cnt, fx in ((1, 5), (2, 6), (4, 7)):
+            c = res[:, cnt].astype(np.float64)
+            if self._weighted.any():
+                c = np.where(self._weighted, res[:, fx].astype(np.float64) * _lib.FX_SCALE, c)
+            out.append(c)
+        return out
 
     def collect(self):
         """Copy results to the host; returns one dict per block (synchronises)."""
@@ -211,9 +243,10 @@ class BlockPlan:
         cols = {k: stats[:, k].tolist() for k in (_lib.STAT_SPHERE, _lib.STAT_BOX, _lib.STAT_GRAZING,
                                                   _lib.STAT_FALLBACK, _lib.STAT_QUERIES)}
         wl = w.tolist()
-        pa_same = (w * res[:, 1].astype(np.float64)).tolist()
-        tail = (2 * w * res[:, 2].astype(np.float64)).tolist()
-        pa_area = (w * res[:, 4].astype(np.float64)).tolist()
+        hits_w, unres_w, pa_w = self._weighted_counts(res)
+        pa_same = (w * hits_w).tolist()
+        tail = (2 * w * unres_w).tolist()
+        pa_area = (w * pa_w).tolist()
         sph, box, graz, fall, qry = (cols[k] for k in (_lib.STAT_SPHERE, _lib.STAT_BOX, _lib.STAT_GRAZING,
                                                       _lib.STAT_FALLBACK, _lib.STAT_QUERIES))
         out = []

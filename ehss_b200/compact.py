@@ -139,6 +139,37 @@ class CompactBoundary:
                                                 ptr(w), stream_handle(dev)), 'compact source')
         return o, d, w
 
+    def max_projected_area(self):
+        """Largest projected area over all directions, widened by 1e-9 so that
+        every ray's weight times ray count stays below it (the reference weight
+        of fused boundary blocks): pi r^2 for the sphere, pi a b for the
+        ellipsoid's two largest semi-axes, |(A_x, A_y, A_z)| for a box with face
+        areas A_k (the maximum of sum_k |d_k| A_k over unit d)."""
+        ax = np.sort(np.asarray(self.axes, dtype=np.float64))[::-1]
+        if self.kind == 'sphere':
+            area = np.pi * ax[0] * ax[0]
+        elif self.kind == 'ellipsoid':
+            area = np.pi * ax[0] * ax[1]
+        else:
+            faces = 4 * np.prod(self.axes) / np.asarray(self.axes, dtype=np.float64)
+            area = float(np.sqrt(np.sum(faces * faces)))
+        return float(area) * (1 + 1e-9)
+
+    def fill_ray_buffer(self, power, seed, buf):
+        """Write the 2**power rays into one float64 device tensor laid out as
+        origins [3n], directions [3n], weights [n] (the ray buffer of a fused
+        boundary block)."""
+        n = 1 << int(power)
+        if buf.numel() < 7 * n:
+            raise ValueError('ray buffer holds fewer than 7 * 2**power values')
+        lib = _lib.load()
+        b = _lib.Boundary(KINDS[self.kind], 0, (ct.c_double * 3)(*self.center),
+                          (ct.c_double * 9)(*np.asarray(self.rotation, dtype=np.float64).ravel()),
+                          (ct.c_double * 3)(*self.axes))
+        p = buf.data_ptr()
+        _lib.check(lib.ehss_compact_source_rays(ct.byref(b), int(power), int(seed), 0, n, p, p + 24 * n, p + 48 * n,
+                                                stream_handle(buf.device)), 'compact source')
+
     def source(self, power, seed):
         """EHSSSource of 2**power rays (CompactBoundary.source, ehss_compact_source.py:47-87)."""
         o, d, w = self.device_rays(power, seed)

@@ -287,6 +287,16 @@ int ehss_blocks_prepare(ehss_block* blocks, int n_blocks, const uint64_t* seeds,
             set_error("block %d: no coherent enumeration", b);
             return EHSS_ERR_VALUE;
         }
+        if (B.flags & EHSS_BLOCK_RAYS) {
+            if (!B.rays || !(B.ray_scale > 0.) || !std::isfinite(B.ray_scale)) {
+                set_error("block %d: ray blocks need a ray buffer and a positive ray_scale", b);
+                return EHSS_ERR_VALUE;
+            }
+        } else {
+            B.rays = nullptr;
+            B.ray_scale = 0.;
+        }
+        if (B.flags & ~(EHSS_BLOCK_EHSS | EHSS_BLOCK_PA | EHSS_BLOCK_RAYS)) { set_error("block %d: unknown flags", b); return EHSS_ERR_VALUE; }
         B.reserved = 0;
         B.chunk_begin = total;
         int64_t n = 1ll << B.log2_rays;
@@ -329,6 +339,10 @@ static int trace_blocks_impl(const ehss_block* blocks_dev, int n_blocks, int64_t
     }
     if (L.resolve_batch < 1 || L.resolve_batch > 32) { set_error("resolve_batch must be 1..32"); return EHSS_ERR_VALUE; }
     if (L.precisions < 0 || L.precisions > 3) { set_error("precisions must be a mask of 1 and 2 (0 = both)"); return EHSS_ERR_VALUE; }
+    if (L.options & ~(EHSS_LAUNCH_COUNT_TESTS | EHSS_LAUNCH_RAY_BLOCKS | EHSS_LAUNCH_NO_DISK_BLOCKS)) {
+        set_error("unknown launch options 0x%x", L.options);
+        return EHSS_ERR_VALUE;
+    }
     cudaStream_t s = as_stream(stream);
     int rc = cuda_status(cudaMemsetAsync(results_dev, 0, sizeof(ehss_block_result) * (size_t)n_blocks, s), "result reset");
     if (!rc && hist_entries > 0) rc = cuda_status(cudaMemsetAsync(hist_dev, 0, 8ull * hist_entries, s), "hist reset");

@@ -63,7 +63,7 @@ struct alignas(256) SceneHeader {
 };
 static_assert(sizeof(SceneHeader) == 256, "scene header is one 256-byte line");
 static_assert(sizeof(ehss_residual) == 88 && offsetof(ehss_residual, block) == 72, "residual ray record layout");
-static_assert(sizeof(ehss_block) % 16 == 0 && offsetof(ehss_block, basis) == 0 && offsetof(ehss_block, base) == 480,
+static_assert(sizeof(ehss_block) == 560 && offsetof(ehss_block, basis) == 0 && offsetof(ehss_block, base) == 480,
               "block descriptors are read with 16-byte vector loads");
 
 struct SceneView {

@@ -473,6 +473,7 @@ struct WarpAcc {
     unsigned hits, unresolved, escaped, pa;
     unsigned queries, grazing, fallback, fp64, errors, pad;
     unsigned long long box, sphere;
+    unsigned long long hits_fx, unres_fx, pa_fx;   // weighted sums of ray blocks
     uint4 q0;
 };
 
@@ -664,7 +665,9 @@ __device__ __forceinline__ bool next_chunk(unsigned long long* counters, int n_p
     return false;
 }
 
-template <bool EXACT, bool COUNT>
+// RAYS: the instance for blocks with EHSS_BLOCK_RAYS (caller-made weighted rays);
+// each instance skips the other kind's chunks, like the precision instances.
+template <bool EXACT, bool COUNT, bool RAYS>
 __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
                                                    int chunk_rays, int resolve_batch, ehss_block_result* results,
                                                    uint64_t* hist, uint64_t* ledger, unsigned long long* work,
@@ -675,6 +678,8 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
     WarpAcc& A = reinterpret_cast<WarpAcc*>(smem_raw)[warp];
     LaneRay& L = reinterpret_cast<LaneRay*>(smem_raw + sizeof(WarpAcc) * nwarps)[threadIdx.x];
     int2* stack_base = reinterpret_cast<int2*>(smem_raw + sizeof(WarpAcc) * nwarps + sizeof(LaneRay) * blockDim.x);
+    // RAYS: each lane's ray weight relative to the block's largest, after the stack
+    double* rho_lane = reinterpret_cast<double*>(stack_base + smem_stack * blockDim.x) + threadIdx.x;
     const unsigned lt_mask = (1u << lane) - 1u;
     Walker<EXACT, COUNT> W;
     W.sstack = stack_base + threadIdx.x;
@@ -695,6 +700,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
         }
         const ehss_block* B = blocks + bi;
         if ((B->precision == EHSS_PREC_FP64) != EXACT) continue;     // the other instantiation's chunk
+        if (((B->flags & EHSS_BLOCK_RAYS) != 0) != RAYS) continue;
         const int cap = B->cap;
         const uint32_t flags = B->flags;
         const int64_t ray0 = (c - B->chunk_begin) * (int64_t)chunk_rays;
@@ -710,6 +716,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
             A.queries = A.grazing = A.fallback = A.fp64 = 0;
             A.errors = ok ? 0 : 1;
             A.box = A.sphere = 0;
+            A.hits_fx = A.unres_fx = A.pa_fx = 0;
         }
         __syncwarp();
         if (COUNT) { W.box = 0; W.sphere = 0; }
@@ -744,15 +751,19 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                     unsigned long long fx = 0;
                     if (escaped) {
                         double a = scatter_angle(L.din[0], L.din[1], L.din[2], L.d[0], L.d[1], L.d[2]);
-                        fx = __double2ull_rn(a * kFxScale);
+                        fx = __double2ull_rn((RAYS ? a * *rho_lane : a) * kFxScale);
                         atomicAdd(&A.escaped, 1u);
                         if (fx) atomicAdd(&A.angle_fx, fx);
                     } else {
                         atomicAdd(&A.unresolved, 1u);
+                        if (RAYS) atomicAdd(&A.unres_fx, __double2ull_rn(*rho_lane * kFxScale));
                         // save the state for a later cap extension
                         if (residual) save_residual(residual, residual_capacity, residual_count, L, bi, last_rank, bounces);
                     }
-                    if (bounces > 0 || !escaped) atomicAdd(&A.hits, 1u);
+                    if (bounces > 0 || !escaped) {
+                        atomicAdd(&A.hits, 1u);
+                        if (RAYS) atomicAdd(&A.hits_fx, __double2ull_rn(*rho_lane * kFxScale));
+                    }
                     if (bounces < kSmemBins) {
                         atomicAdd(&A.count[bounces], 1u);
                         if (fx) atomicAdd(&A.ledger[bounces], fx);
@@ -778,14 +789,29 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                 if (status == kNeedRay) {
                     int p = pool + __popc(need & lt_mask);
                     if (p < cnt) {
-                        // ray0 is a multiple of the chunk size, so point(ray0 + p) = point(ray0) ^ B(p)
-                        uint4 q = block_point(reinterpret_cast<const uint4*>(B->basis), A.q0, (uint32_t)p);
-                        Ray64 ray = impact_ray(q, S.h->center, S.h->radius);
+                        if (RAYS) {
+                            // caller-made rays: origins [3n], directions [3n], weights [n]
+                            const int64_t n = 1ll << B->log2_rays, r = ray0 + p;
+                            const double* R = B->rays;
 #pragma unroll
-                        for (int i = 0; i < 3; ++i) { L.o[i] = ray.o[i]; L.d[i] = ray.d[i]; L.din[i] = ray.d[i]; }
+                            for (int i = 0; i < 3; ++i) {
+                                L.o[i] = R[3 * r + i];
+                                L.d[i] = L.din[i] = R[3 * n + 3 * r + i];
+                            }
+                            *rho_lane = R[6 * n + r] * B->ray_scale;
+                        } else {
+                            // ray0 is a multiple of the chunk size, so point(ray0 + p) = point(ray0) ^ B(p)
+                            uint4 q = block_point(reinterpret_cast<const uint4*>(B->basis), A.q0, (uint32_t)p);
+                            Ray64 ray = impact_ray(q, S.h->center, S.h->radius);
+#pragma unroll
+                            for (int i = 0; i < 3; ++i) { L.o[i] = ray.o[i]; L.d[i] = ray.d[i]; L.din[i] = ray.d[i]; }
+                        }
                         if (flags & EHSS_BLOCK_PA) {
                             LocalStats pst;
-                            if (anyhit(S, L.o, L.d, -1, pst)) atomicAdd(&A.pa, 1u);
+                            if (anyhit(S, L.o, L.d, -1, pst)) {
+                                atomicAdd(&A.pa, 1u);
+                                if (RAYS) atomicAdd(&A.pa_fx, __double2ull_rn(*rho_lane * kFxScale));
+                            }
                         }
                         bounces = 0;
                         last_rank = -1;
@@ -845,6 +871,9 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
             if (A.unresolved) atomicAdd((unsigned long long*)&R->unresolved, (unsigned long long)A.unresolved);
             if (A.escaped) atomicAdd((unsigned long long*)&R->escaped, (unsigned long long)A.escaped);
             if (A.pa) atomicAdd((unsigned long long*)&R->pa_blocked, (unsigned long long)A.pa);
+            if (A.hits_fx) atomicAdd((unsigned long long*)&R->hits_fx, A.hits_fx);
+            if (A.unres_fx) atomicAdd((unsigned long long*)&R->unresolved_fx, A.unres_fx);
+            if (A.pa_fx) atomicAdd((unsigned long long*)&R->pa_fx, A.pa_fx);
             unsigned long long v[7] = {A.box, A.sphere, A.queries, A.grazing, A.fallback, A.fp64, A.errors};
             const int slot[7] = {EHSS_STAT_BOX_TESTS, EHSS_STAT_SPHERE_TESTS, EHSS_STAT_QUERIES, EHSS_STAT_GRAZING,
                                  EHSS_STAT_FALLBACK, EHSS_STAT_FP64_TESTS, EHSS_STAT_ERRORS};
@@ -905,32 +934,42 @@ int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const 
                   unsigned long long* residual_count) {
     int warps = L.block_threads / 32;
     const int sdepth = L.smem_stack > 0 ? L.smem_stack : 16;
-    size_t smem = sizeof(WarpAcc) * (size_t)warps + sizeof(LaneRay) * (size_t)L.block_threads +
-                  sizeof(int2) * sdepth * (size_t)L.block_threads;
+    const size_t smem = sizeof(WarpAcc) * (size_t)warps + sizeof(LaneRay) * (size_t)L.block_threads +
+                        sizeof(int2) * sdepth * (size_t)L.block_threads;
+    const size_t smem_rays = smem + sizeof(double) * (size_t)L.block_threads;
     unsigned grid = (unsigned)(sm_count() * L.ctas_per_sm);
     int batch = L.resolve_batch > 0 ? L.resolve_batch : 1;
     const bool count = (L.options & EHSS_LAUNCH_COUNT_TESTS) != 0;
-    // one launch per precision present; each skips the other precision's chunks
+    // one launch per precision and ray kind present; each skips the other blocks' chunks
     const int mask = L.precisions ? L.precisions : 3;
+    const int kinds = (L.options & EHSS_LAUNCH_RAY_BLOCKS) ? ((L.options & EHSS_LAUNCH_NO_DISK_BLOCKS) ? 2 : 3) : 1;
     bool first = true;
     for (int exact = 1; exact >= 0; --exact) {
         if (!((mask >> (exact ? EHSS_PREC_FP64 : EHSS_PREC_FP32)) & 1)) continue;
-        if (!first) {
-            int rc = cuda_status(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * kMaxWorkParts, stream),
-                                 "work counter reset");
+        for (int rays = 0; rays <= 1; ++rays) {
+            if (!((kinds >> rays) & 1)) continue;
+            if (!first) {
+                int rc = cuda_status(cudaMemsetAsync(work, 0, sizeof(unsigned long long) * kMaxWorkParts, stream),
+                                     "work counter reset");
+                if (rc) return rc;
+            }
+            first = false;
+            const int n_parts = sm_count() < kMaxWorkParts ? sm_count() : kMaxWorkParts;
+#define EHSS_LAUNCH_BLOCKS(E, C, R) \
+            k_blocks<E, C, R><<<grid, L.block_threads, R ? smem_rays : smem, stream>>>( \
+                blocks, nb, total_chunks, L.chunk_rays, batch, results, hist, ledger, work, n_parts, sdepth, \
+                residual, residual_capacity, residual_count)
+            if (exact) {
+                if (rays) { if (count) EHSS_LAUNCH_BLOCKS(true, true, true); else EHSS_LAUNCH_BLOCKS(true, false, true); }
+                else { if (count) EHSS_LAUNCH_BLOCKS(true, true, false); else EHSS_LAUNCH_BLOCKS(true, false, false); }
+            } else {
+                if (rays) { if (count) EHSS_LAUNCH_BLOCKS(false, true, true); else EHSS_LAUNCH_BLOCKS(false, false, true); }
+                else { if (count) EHSS_LAUNCH_BLOCKS(false, true, false); else EHSS_LAUNCH_BLOCKS(false, false, false); }
+            }
+#undef EHSS_LAUNCH_BLOCKS
+            int rc = cuda_status(cudaGetLastError(), "blocks launch");
             if (rc) return rc;
         }
-        first = false;
-        const int n_parts = sm_count() < kMaxWorkParts ? sm_count() : kMaxWorkParts;
-#define EHSS_LAUNCH_BLOCKS(E, C) \
-        k_blocks<E, C><<<grid, L.block_threads, smem, stream>>>(blocks, nb, total_chunks, L.chunk_rays, batch, \
-                                                                results, hist, ledger, work, n_parts, sdepth, \
-                                                                residual, residual_capacity, residual_count)
-        if (exact) { if (count) EHSS_LAUNCH_BLOCKS(true, true); else EHSS_LAUNCH_BLOCKS(true, false); }
-        else { if (count) EHSS_LAUNCH_BLOCKS(false, true); else EHSS_LAUNCH_BLOCKS(false, false); }
-#undef EHSS_LAUNCH_BLOCKS
-        int rc = cuda_status(cudaGetLastError(), "blocks launch");
-        if (rc) return rc;
     }
     return EHSS_OK;
 }
@@ -955,7 +994,7 @@ __global__ void __launch_bounds__(128) k_extend(const ehss_block* blocks, int nb
         if (row >= rows) { ++st.errors; continue; }
         const ehss_block* B = blocks + R.block;
         const SceneView S = scene_view(B->scene);
-        if (S.h->magic != kSceneMagic || S.h->status != 0 || R.bounces >= new_cap || R.last_rank < -1 ||
+        if ((B->flags & EHSS_BLOCK_RAYS) || S.h->magic != kSceneMagic || S.h->status != 0 || R.bounces >= new_cap || R.last_rank < -1 ||
             R.last_rank >= S.h->n_atoms) {
             ++st.errors;
             continue;

@@ -228,8 +228,14 @@ int ehss_pa_grid(const void* scene_dev, int64_t n_atoms, int n_dirs, uint64_t se
  * weighted by the contribution in 2^-36 units). */
 #define EHSS_BLOCK_EHSS 1u      /* trace EHSS */
 #define EHSS_BLOCK_PA 2u        /* any-hit PA on the same rays */
+#define EHSS_BLOCK_RAYS 4u      /* rays from `rays` (origins [3n], directions [3n], weights [n],
+                                   float64, n = 2^log2_rays; e.g. ehss_compact_source_rays) instead
+                                   of the scene's impact disk: every ray then adds its weight
+                                   times ray_scale (<= 1 + 1e-9) to the weighted sums hits_fx,
+                                   unresolved_fx, pa_fx and to angle_fx, and
+                                   omega = angle_fx * 2^-36 / ray_scale etc. */
 
-/* 544 bytes, a multiple of 16: the device reads basis/base as 16-byte
+/* 560 bytes, a multiple of 16: the device reads basis/base as 16-byte
  * vectors, so a device array of blocks must start on a 16-byte boundary.
  * ehss_blocks_prepare fills basis/base with the block's 2^log2_rays Sobol(4)
  * points of `seed` in a spatially coherent enumeration: position p carries
@@ -248,6 +254,8 @@ typedef struct ehss_block {
     uint32_t flags;           /* EHSS_BLOCK_* */
     int64_t hist_offset;      /* first hist/ledger entry of this block (-1: next free) */
     int64_t chunk_begin;      /* filled by ehss_blocks_prepare */
+    const double* rays;       /* EHSS_BLOCK_RAYS: device ray buffer, else NULL */
+    double ray_scale;         /* EHSS_BLOCK_RAYS: 1 / (largest ray weight), else 0 */
     int64_t reserved;         /* 0 */
 } ehss_block;
 
@@ -257,6 +265,9 @@ typedef struct ehss_block_result {
     uint64_t unresolved;
     uint64_t escaped;
     uint64_t pa_blocked;      /* any-hit PA count (EHSS_BLOCK_PA) */
+    uint64_t hits_fx;         /* EHSS_BLOCK_RAYS: weighted hits, unresolved rays and PA hits, */
+    uint64_t unresolved_fx;   /*   each ray adding weight * ray_scale in 2^-36 units */
+    uint64_t pa_fx;
     uint64_t stats[EHSS_NSTATS];
 } ehss_block_result;
 
@@ -283,6 +294,8 @@ typedef struct ehss_launch {
     int32_t reserved;         /* 0 */
 } ehss_launch;
 #define EHSS_LAUNCH_COUNT_TESTS 1   /* count box and sphere tests into the block stats (slower) */
+#define EHSS_LAUNCH_RAY_BLOCKS 2    /* some blocks have EHSS_BLOCK_RAYS (adds a launch of that kernel instance) */
+#define EHSS_LAUNCH_NO_DISK_BLOCKS 4  /* with EHSS_LAUNCH_RAY_BLOCKS: every block has EHSS_BLOCK_RAYS */
 
 /* Run all blocks in one persistent launch.  blocks_dev: device copy of the
  * prepared descriptors; results_dev[n_blocks], hist_dev/ledger_dev

@@ -97,3 +97,30 @@ def test_boundary_validation(eb):
         b.source(-1, 0)
     with pytest.raises(ValueError):
         b.source(3, -5)
+
+
+@pytest.mark.parametrize('kind', ['box', 'ellipsoid', 'sphere'])
+def test_fused_boundary_blocks_match_explicit_trace(eb, kind):
+    """Boundary rays in the fused kernel (EHSS_BLOCK_RAYS, weighted fixed-point
+    sums) against the same rays traced one by one and read out on the host."""
+    from ehss_b200 import workloads as W
+    from ehss_b200.batch import BatchCCS
+    structures = [W.globule(n, 60 + n)[:2] for n in (40, 900)]
+    bc = BatchCCS(structures, 12, [7, 8], repeats=2, cap=32, pa=True, graph=False, boundary=kind)
+    out = bc.run()
+    for (c, r), o in zip(structures, out):
+        s = eb.Spheres(c, r, deduplicate=False)
+        prep = eb.PreparedStaticGPUEHSS(s, boundary=kind)
+        for run in o['runs']:
+            seed = bc.plan.jobs[o['structure'] * 2 + run['tag'][1]].seed
+            src = prep.boundary.source(12, seed)
+            ref = prep.engine.trace(src, 32)
+            assert run['ehss_angstrom2'] == pytest.approx(ref.omega, rel=1e-11)
+            assert run['tail_bound_angstrom2'] == pytest.approx(ref.tail_bound, rel=1e-11, abs=1e-12)
+            assert run['pa_from_same_rays_angstrom2'] == pytest.approx(ref.pa, rel=1e-11)
+            assert run['collision_histogram'] == np.bincount(ref.bounces, minlength=33).tolist()
+            assert run['unresolved_rays'] == int(ref.unresolved.sum())
+            hit = O.PATree(c, r, 4).query(src.origins, src.directions)[0]
+            assert run['pa_angstrom2'] == pytest.approx(float(src.weights[hit].sum()), rel=1e-11)
+    with pytest.raises(ValueError):
+        BatchCCS(structures, 12, [7, 8], boundary=kind, cap_ladder=(64,))

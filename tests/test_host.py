@@ -98,8 +98,8 @@ def test_blocks_prepare_chunks_and_offsets(lib):
 
 def test_struct_layouts_match_header():
     from ehss_b200 import _lib
-    assert ct.sizeof(_lib.Block) == 544 and _lib.Block.basis.offset == 0 and _lib.Block.base.offset == 480
-    assert ct.sizeof(_lib.BlockResult) == 8 * (5 + _lib.NSTATS)
+    assert ct.sizeof(_lib.Block) == 560 and _lib.Block.basis.offset == 0 and _lib.Block.base.offset == 480
+    assert ct.sizeof(_lib.BlockResult) == 8 * (8 + _lib.NSTATS)
     assert ct.sizeof(_lib.Launch) == 32
     assert ct.sizeof(_lib.SceneInfo) == 96 and _lib.SceneInfo.n_active.offset == 80
 
