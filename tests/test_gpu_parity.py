@@ -393,3 +393,68 @@ def test_cli_all_frames_batched_equals_per_frame(eb, tmp_path):
         for a, b in zip(rec['runs'], one['runs']):
             assert a['ehss']['collision_histogram'] == b['ehss']['collision_histogram']
             assert a['ehss']['collision_contribution_angstrom2'] == b['ehss']['collision_contribution_angstrom2']
+
+
+# ---- the benchmark's parity configurations -------------------------------------------------
+def test_config_triatomic_rotated_repeats(eb):
+    """Bent triatomic, 4096 rays x seeds 0-2, the geometry rotated by a uniform
+    SO(3) rotation seeded per repeat (the reference has no rotation option, so
+    the same rotation is applied to the atoms for the oracle and the device)."""
+    from ehss_b200 import workloads as W
+    from ehss_b200.blocks import BlockJob, BlockPlan
+    c0, r, _ = W.triatomic()
+    for seed in (0, 1, 2):
+        c = c0 @ W.random_rotation(seed).T
+        scene = eb.Scene(c, r)
+        plan = BlockPlan([BlockJob(scene, 12, seed, cap=64, precision=0, pa=True)])
+        plan.run()
+        got = plan.collect()[0]
+        o, d = (x.cpu().numpy() for x in scene.source_rays(12, seed))
+        ref = O.StaticTree(c, r, 4).trace(o, d, cap=64, threads=O.host_cores())
+        ro = O.readout(dict(incoming=d, weights=np.full(len(o), np.pi * scene.radius ** 2 / len(o))), ref, 64)
+        assert got['ehss_angstrom2'] == pytest.approx(ro['ehss_angstrom2'], rel=CCS_RTOL)
+        assert got['collision_histogram'] == ro['collision_histogram']
+        hits, _, _ = O.PATree(c, r, 4).query(o, d, threads=O.host_cores())
+        assert got['pa_blocked_rays'] == int(hits.sum())
+
+
+def test_config_globule650_fp64_per_ray_20_seeds(eb):
+    """650-atom globule, 65,536 rays x 20 seeds in FP64 on the device: every
+    ray's outcome, bounce count and outgoing direction equal the oracle's, and
+    so do the BVH-PA hit flags."""
+    from ehss_b200 import workloads as W
+    c, r, _ = W.globule(650, 650)
+    s = eb.Spheres(c, r, deduplicate=False)
+    prep = eb.PreparedStaticGPUEHSS(s, precision='fp64')
+    index = eb.SphereIndex(s)
+    tree, patree = O.StaticTree(c, r, 4), O.PATree(c, r, 4)
+    for seed in range(20):
+        src = eb.external_source(s, 16, seed, scene=prep.scene)
+        got = prep.engine.trace(src, 64)
+        ref = tree.trace(src.origins, src.directions, cap=64, threads=O.host_cores())
+        for field in ('outgoing', 'escaped', 'unresolved', 'bounces'):
+            np.testing.assert_array_equal(getattr(got, field), ref[field], err_msg=f'seed {seed} {field}')
+        blocked, _, _ = index.query(src)
+        np.testing.assert_array_equal(blocked, patree.query(src.origins, src.directions, threads=O.host_cores())[0])
+
+
+def test_config_globule2000_fp32_precision(eb):
+    """2000-atom globule, 262,144 rays per seed through the fused FP32 kernel
+    with FP64 re-test: CCS within 1e-12 of the FP64 oracle on the same rays,
+    identical bounce histograms, grazing queries counted."""
+    from ehss_b200 import workloads as W
+    from ehss_b200.blocks import BlockJob, BlockPlan, DEFAULT_LAUNCH
+    c, r, _ = W.globule(2000, 2000)
+    scene = eb.Scene(c, r, exterior=True)
+    tree = O.StaticTree(c, r, 4)
+    for seed in (0, 1):
+        plan = BlockPlan([BlockJob(scene, 18, seed, cap=64)], launch=dict(DEFAULT_LAUNCH, count_tests=True))
+        plan.run()
+        got = plan.collect()[0]
+        o, d = (x.cpu().numpy() for x in scene.source_rays(18, seed))
+        ref = tree.trace(o, d, cap=64, threads=O.host_cores())
+        ro = O.readout(dict(incoming=d, weights=np.full(len(o), np.pi * scene.radius ** 2 / len(o))), ref, 64)
+        assert abs(got['ehss_angstrom2'] - ro['ehss_angstrom2']) <= 1e-12 * ro['ehss_angstrom2']
+        assert got['collision_histogram'] == ro['collision_histogram']
+        assert got['unresolved_rays'] == ro['unresolved_rays']
+        assert got['grazing_queries'] >= 0 and got['queries'] > len(o)
