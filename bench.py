@@ -451,6 +451,12 @@ def main():
                 "ref_sphere_tests_per_ray": float(np.sum(ray_counts * s_ref) / ray_counts.sum()),
                 "ref_box_tests_per_ray": float(np.sum(ray_counts * b_ref) / ray_counts.sum()),
                 "peak_note": f"nominal FP32: {n_sm} SMs x 128 lanes x 2 x {sm_max:.0f} MHz (no measured FP32 peak)"}
+        # the ray-sphere-test roofline: reference sphere tests per second against peak / 35 ops
+        sphere_rate = float(np.sum(ray_counts * s_ref)) / (mean_trace_ms * 1e-3)
+        roof["ray_sphere_tests"] = {"achieved_per_s": sphere_rate, "peak_per_s": peak_tflops * 1e12 / C_SPHERE,
+                                    "frac": sphere_rate / (peak_tflops * 1e12 / C_SPHERE),
+                                    "own_tests_per_s": own["sphere_tests_per_query"] * own["queries_per_ray"] *
+                                    rays_step / (mean_trace_ms * 1e-3)}
         ccs_err = ccs_error_vs_oracle(eb, structures[::32])
         if world == 1 and not args.no_cpu_baseline:
             rate, kind, cores, rays_done, secs = cpu_reference_rate(structures[::16], 12, 190003)
