@@ -139,6 +139,7 @@ int ehss_scenes_workspace_bytes(int n_scenes, const int64_t* n_atoms_host, uint6
         if (n_atoms_host[s] < 1) { set_error("structure %d has no atoms", s); return EHSS_ERR_VALUE; }
         N += n_atoms_host[s];
     }
+    if (N > (int64_t)INT32_MAX) { set_error("a batch holds at most %d atoms", INT32_MAX); return EHSS_ERR_VALUE; }
     *workspace_bytes = build_workspace_bytes(N, n_scenes);
     return EHSS_OK;
 }

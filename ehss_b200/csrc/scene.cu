@@ -882,6 +882,11 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
         N += n[s];
         I += n[s] - 1;
     }
+    if (N > (int64_t)INT32_MAX) {          // the key sort counts items in int
+        delete[] host;
+        set_error("a batch holds at most %d atoms, got %lld", INT32_MAX, (long long)N);
+        return EHSS_ERR_VALUE;
+    }
     uint64_t need = build_workspace_bytes(N, S);
     if (workspace_bytes < need) {
         delete[] host;

@@ -60,6 +60,9 @@ def test_argument_validation_without_device(lib):
     assert lib.ehss_scenes_build_ex(1, one, one, (ct.c_int64 * 1)(10), 8, one, (ct.c_uint64 * 1)(1 << 20), 1024,
                                     1 << 20, 2, None) == _lib.ERR_VALUE
     assert b'unknown build flags' in lib.ehss_last_error()
+    wb = ct.c_uint64()
+    assert lib.ehss_scenes_workspace_bytes(3, (ct.c_int64 * 3)(1 << 30, 1 << 30, 1 << 30), ct.byref(wb)) == _lib.ERR_VALUE
+    assert b'at most' in lib.ehss_last_error()
     assert lib.ehss_scenes_build_ex(0, one, one, (ct.c_int64 * 1)(10), 8, one, (ct.c_uint64 * 1)(1 << 20), 1024,
                                     1 << 20, 1, None) == _lib.ERR_VALUE
     with pytest.raises(ValueError):
