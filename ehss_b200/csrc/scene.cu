@@ -622,17 +622,31 @@ __global__ void __launch_bounds__(32 * kExposureWarps, 4) k_exposure(BuildDesc* 
             __syncwarp();
             cur ^= 1;
         }
-        // 2. neighbours with a cap on the finest lattice; lanes split over leaves of <= 8 or <= 16 atoms
+        // 2. neighbours with a cap on the finest lattice: the atoms of all listed leaves, one per lane
         const int nl = min(W.n_leaves, kLeafList);
-        const int per_leaf = S.h->leaf_size <= 8 ? 8 : 16, leaves_per_pass = 32 / per_leaf;
-        const int slot_in_leaf = lane % per_leaf;
-        for (int base = 0; base < nl; base += leaves_per_pass) {
-            const int l = base + lane / per_leaf;
-            if (l >= nl) continue;
-            const int code = ~W.leaves[l];
-            const int first = code >> kLeafBits, cnt = (code & (kMaxLeaf - 1)) + 1;
-            const int k = first + slot_in_leaf;
-            if (slot_in_leaf >= cnt || k >= S.h->n_atoms || k == j) continue;
+        int* leaf_end = W.front[0];                 // free after the walk: running atom counts of the leaves
+        int n_cand = 0;
+        for (int base = 0; base < nl; base += 32) {
+            const int l = base + lane;
+            const int c = l < nl ? ((~W.leaves[l]) & (kMaxLeaf - 1)) + 1 : 0;
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(full, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (l < nl) leaf_end[l] = n_cand + incl;
+            n_cand += __shfl_sync(full, incl, 31);
+        }
+        __syncwarp();
+        for (int t = lane; t < n_cand; t += 32) {
+            int lo_l = 0, hi_l = nl - 1;                // leaf of candidate t: first with leaf_end > t
+            while (lo_l < hi_l) {
+                const int mid = (lo_l + hi_l) >> 1;
+                if (leaf_end[mid] > t) hi_l = mid; else lo_l = mid + 1;
+            }
+            const int k = ((~W.leaves[lo_l]) >> kLeafBits) + t - (lo_l ? leaf_end[lo_l - 1] : 0);
+            if (k >= S.h->n_atoms || k == j) continue;
             const float4 a = S.atoms[k];
             const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
             const float d = sqrtf(dx * dx + dy * dy + dz * dz);
