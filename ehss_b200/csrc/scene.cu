@@ -25,8 +25,14 @@
 //                  leaf_size atoms collapsed into leaf references; per atom:
 //                  FP32 and FP64 atom records in leaf order, id maps.
 #include <cub/device/device_radix_sort.cuh>
+#include <algorithm>
+#include <array>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
 #include "ehss_internal.cuh"
 
 namespace ehss {
@@ -434,49 +440,54 @@ __global__ void k_fill_scene_index(const BuildDesc* descs, int n_scenes, int32_t
 //
 // Test (one warp per atom B, radius r).  Each neighbour C overlapping B gives
 // a cap on B's unit sphere, {s : |r s - (c_C - c_B)| <= r_C - h - mu}, i.e.
-// s.u_C >= cos(alpha_C) with u_C the unit direction to C.  Lattice K is the
-// latitude lattice with rows theta_k = (k + 1/2) pi / K and ceil(2 K sin
-// theta_k) + 1 points per row; its geodesic covering radius is at most pi / K.
-// A sample of lattice K is "covered" when it lies in some cap with h = r pi /
-// K: every surface point within geodesic pi / K of it is then inside C at
-// depth >= mu.  B is buried when every surface point is certified that way:
-//   level 0: every sample of lattice 12 is tested; the uncovered ones U are
-//            kept.  A point is certified unless it lies within pi / 12 of
-//            some U.
-//   level i: lattice K = 12 * 2^i is tested only within geodesic 3 pi / K of
-//            each U of the previous level (every point within pi / (K / 2) of
-//            U has its nearest lattice-K sample there); the uncovered ones
-//            become the next U.  No U left: buried.
-// Levels stop at K = 48; more than kMaxOpen open samples, or any left at the
-// last level, keep the atom (deeper levels and more open samples cut more
-// atoms but cost more build time than they save in the trace of one batch).  mu = 1e-4 (r + d + r_C) + 2e-6 S bounds the
-// FP32 error of the cap test (at most 1e-5 (r + d + r_C) for the caps used,
-// whose shrunk radius is >= 0.05 (r + d + r_C)) and of the FP32 atom records
-// ten times over; the candidate search is widened by 5 % and one sample per
-// row so that rounding cannot drop a sample.  Dropping a neighbour, or
-// declaring an atom exposed, only keeps atoms, so the fixed-size lists below
-// never make a wrong cut.
+// s.u_C >= cos(alpha_C) with u_C the unit direction to C.  The samples are
+// the vertices of the geodesic (icosahedral) spheres of 162, 642 and 2562
+// vertices (levels A, B, C; each level's vertices start with the previous
+// level's).  Their covering radii rho_L -- the largest distance from a point
+// of the sphere to the nearest vertex, computed on the host from the
+// triangulation (the circumradius of each triangle, or half its longest
+// edge when the circumcentre falls outside) -- bound every surface point's
+// chord distance to its nearest level-L sample by r rho_L.  A sample of level
+// L is "covered" when it lies in some cap with h = r rho_L: every surface
+// point within rho_L of it is then inside C at depth >= mu.  B is buried when
+// every surface point is certified that way:
+//   level A: every vertex is tested; the uncovered ones are kept open.
+//   level B, C: only the vertices within rho_prev + rho_L of an open vertex
+//            of the previous level are tested (every point within rho_prev
+//            of that vertex has its nearest level-L vertex among them, from
+//            host-made neighbour lists); the uncovered ones become the open
+//            vertices.  None open: buried.
+// More than kMaxOpen open vertices, or any left at level C, keep the atom.
+// mu = 1e-4 (r + d + r_C) + 2e-6 S bounds the FP32 error of the cap test (at
+// most 1e-5 (r + d + r_C) for the caps used, whose shrunk radius is >= 0.05
+// (r + d + r_C)), of the FP32 atom records and of the FP32 vertex directions
+// ten times over.  Dropping a neighbour, or declaring an atom exposed, only
+// keeps atoms, so the fixed-size lists below never make a wrong cut.
 // --------------------------------------------------------------------------
-constexpr int kLattice0 = 12;          // the fully tested lattice
-constexpr int kRefineLevels = 2;       // then K = 24, 48 around open samples
-constexpr int kLattice0Max = 256;      // > sum_k (2 K sin theta_k + 2) for K = 12
+constexpr int kIcoA = 162, kIcoB = 642, kIcoC = 2562;
+constexpr int kIcoNbr = 24;            // neighbour list width (at most 17 used: checked on the host)
 constexpr int kExposureWarps = 8;
 constexpr int kMaxCaps = 96;
 constexpr int kFrontier = 64;
 constexpr int kLeafList = 64;
 constexpr int kMaxOpen = 8;
-constexpr int kRefRows = 24 + 48;      // rows of the refinement lattices (K = 24, 48)
-constexpr int kMaskWords = 128;        // > (samples of lattice 48) / 32
-constexpr int kCandList = 256;         // distinct candidate samples of one refinement level
-constexpr float kPi = 3.14159265358979f;
+constexpr int kMaskWords = (kIcoC + 31) / 32;
+constexpr int kCandList = 256;         // distinct candidate vertices of one refinement level
+
+// geodesic sphere vertices (levels A, B, C are prefixes), level A -> B and
+// B -> C neighbour lists, covering radii (uploaded by build_scenes)
+__device__ float4 g_ico_dirs[kIcoC];
+__device__ uint16_t g_ico_nbr[(kIcoA + kIcoB) * kIcoNbr];
+__device__ uint8_t g_ico_nnbr[kIcoA + kIcoB];
+__device__ float g_ico_rho[3];
 
 struct ExposureWarp {
     float4 cap[kMaxCaps];              // (u, cos alpha at the current lattice)
     float2 dr[kMaxCaps];               // (distance, radius of C)
     int front[2][kFrontier];
     int leaves[kLeafList];
-    int open[2][kMaxOpen];             // open samples (row << 16 | index) of the last two levels
-    unsigned mask[kMaskWords];         // candidate samples of the current refinement level
+    int open[2][kMaxOpen];             // open vertices of the last two levels
+    unsigned mask[kMaskWords];         // candidate vertices of the current refinement level
     int cand[kCandList];
     int n_front[2];
     int n_leaves, n_caps, whole;
@@ -487,10 +498,6 @@ __device__ __forceinline__ float cap_cos(float r, float d, float rc_full, float 
     const float rc = rc_full - h - 1e-4f * L - mS;     // shrunk radius of C
     if (rc < 0.05f * L || d >= r + rc) return 3.f;    // too thin to count, or no cap
     return (r * r + d * d - rc * rc) / (2.f * r * d);
-}
-
-__device__ __forceinline__ int lattice_row_len(int K, float theta) {
-    return (int)ceilf(2.0f * K * sinf(theta)) + 1;
 }
 
 // Caps for lattice spacing h; true when one cap alone holds the whole sphere.
@@ -523,53 +530,13 @@ __device__ __forceinline__ bool in_some_cap(const ExposureWarp& W, int nc, float
 
 __global__ void __launch_bounds__(32 * kExposureWarps, 4) k_exposure(BuildDesc* descs, const int32_t* atom_scene,
                                                                   int64_t N, uint8_t* culled) {
-    __shared__ float4 dirs0[kLattice0Max];      // lattice 12: (x, y, z, id bits)
-    __shared__ int row_start0[kLattice0 + 1];
+    __shared__ float4 dirs_a[kIcoA];
     __shared__ ExposureWarp wsm[kExposureWarps];
-    __shared__ int rstart[kRefRows + kRefineLevels];    // per level: K + 1 row starts
-    __shared__ float2 rsc[kRefRows];                    // per level and row: (sin, cos) of theta
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu, below = (1u << lane) - 1u;
-    static_assert(kRefineLevels == 2, "refinement tables are sized for K = 24 and 48");
-    if (threadIdx.x == 32) {
-        for (int lv = 1; lv <= kRefineLevels; ++lv) {
-            const int K = kLattice0 << lv, r0 = kLattice0 * ((1 << lv) - 2), s0 = r0 + lv - 1;
-            int t = 0;
-            for (int k = 0; k < K; ++k) {
-                rstart[s0 + k] = t;
-                t += lattice_row_len(K, (k + 0.5f) * kPi / K);
-            }
-            rstart[s0 + K] = t;
-        }
-    }
-    for (int t = threadIdx.x; t < kRefRows; t += blockDim.x) {
-        const int lv = t < 24 ? 1 : 2, K = kLattice0 << lv, k = t - kLattice0 * ((1 << lv) - 2);
-        float sn, cs;
-        sincosf((k + 0.5f) * kPi / K, &sn, &cs);
-        rsc[t] = make_float2(sn, cs);
-    }
-    if (threadIdx.x == 0) {
-        int t = 0;
-        for (int k = 0; k < kLattice0; ++k) {
-            row_start0[k] = t;
-            t += lattice_row_len(kLattice0, (k + 0.5f) * kPi / kLattice0);
-        }
-        row_start0[kLattice0] = t < kLattice0Max ? t : kLattice0Max;
-    }
+    for (int t = threadIdx.x; t < kIcoA; t += blockDim.x) dirs_a[t] = g_ico_dirs[t];
     __syncthreads();
-    const int n0 = row_start0[kLattice0];
-    for (int t = threadIdx.x; t < n0; t += blockDim.x) {
-        int k = 0;
-        while (k + 1 < kLattice0 && row_start0[k + 1] <= t) ++k;
-        const int l = t - row_start0[k];
-        const int L = row_start0[k + 1] - row_start0[k];
-        float st, ct, sp, cp;
-        sincosf((k + 0.5f) * kPi / kLattice0, &st, &ct);
-        sincosf(2.f * kPi * (float)l / (float)L, &sp, &cp);
-        dirs0[t] = make_float4(st * cp, st * sp, ct, __int_as_float((k << 16) | l));
-    }
-    __syncthreads();
-    const int stride0 = n0 % 97 ? 97 : 89;          // scattered visiting order, coprime to n0
+    const float rho_a = g_ico_rho[0], rho_b = g_ico_rho[1], rho_c = g_ico_rho[2];
     ExposureWarp& W = wsm[warp];
     for (int64_t g = blockIdx.x * (int64_t)kExposureWarps + warp; g < N; g += (int64_t)gridDim.x * kExposureWarps) {
         BuildDesc& D = descs[atom_scene[g]];
@@ -577,7 +544,7 @@ __global__ void __launch_bounds__(32 * kExposureWarps, 4) k_exposure(BuildDesc* 
         const int j = (int)(g - D.atom0);          // leaf-order position: neighbouring warps share subtrees
         const float4 b = S.atoms[j];
         const float mS = 2e-6f * S.h->scale_f;
-        const float h_fine = b.w * kPi / (kLattice0 << kRefineLevels);
+        const float h_fine = b.w * rho_c;
         if (lane == 0) {
             W.front[0][0] = 0;
             W.n_front[0] = 1;
@@ -693,75 +660,44 @@ __global__ void __launch_bounds__(32 * kExposureWarps, 4) k_exposure(BuildDesc* 
             __syncwarp();
         }
         bool exposed = nc == 0 && !buried;
-        // 3a. lattice 12, every sample; open samples recorded
+        // 3a. level A: every vertex; the uncovered ones stay open
         int n_open = 0;
         if (!buried && !exposed) {
-            buried = set_caps(W, nc, b.w, b.w * kPi / kLattice0, mS, lane);
-            for (int base = 0; base < n0 && !buried && !exposed; base += 32) {
+            buried = set_caps(W, nc, b.w, b.w * rho_a, mS, lane);
+            for (int base = 0; base < kIcoA && !buried && !exposed; base += 32) {
                 const int t = base + lane;
                 bool miss = false;
-                int id = 0;
-                if (t < n0) {
-                    const float4 s = dirs0[(int)(((int64_t)t * stride0) % n0)];
+                if (t < kIcoA) {
+                    const float4 s = dirs_a[t];
                     miss = !in_some_cap(W, nc, s.x, s.y, s.z);
-                    id = __float_as_int(s.w);
                 }
                 const unsigned m = __ballot_sync(full, miss);
                 const int at = n_open + __popc(m & below);
-                if (miss && at < kMaxOpen) W.open[0][at] = id;
+                if (miss && at < kMaxOpen) W.open[0][at] = t;
                 n_open += __popc(m);
                 exposed = n_open > kMaxOpen;
             }
             __syncwarp();
             if (!buried && !exposed && n_open == 0) buried = true;
         }
-        // 3b. finer lattices around the open samples: mark the distinct candidates of
-        //     every open sample in a bit mask, then test them once each
+        // 3b. levels B and C: the distinct neighbours of the open vertices, each tested once
         int side = 0;
-        for (int lv = 1; lv <= kRefineLevels && !buried && !exposed; ++lv) {
-            const int K = kLattice0 << lv, Kp = K >> 1;
-            const int r0 = kLattice0 * ((1 << lv) - 2);          // first row of this level in rsc
-            const int* rs = rstart + r0 + lv - 1;                // its K + 1 row starts
-            const int n_k = rs[K], words = (n_k + 31) >> 5;
-            const float alpha = 1.05f * 3.f * kPi / K;            // 3 pi / K, widened
-            const float ca = cosf(alpha);
-            if (set_caps(W, nc, b.w, b.w * kPi / K, mS, lane)) { buried = true; break; }
+        for (int lv = 1; lv <= 2 && !buried && !exposed; ++lv) {
+            const int n_lv = lv == 1 ? kIcoB : kIcoC, words = (n_lv + 31) >> 5;
+            const int nbr0 = lv == 1 ? 0 : kIcoA;           // neighbour lists of the previous level's vertices
+            if (set_caps(W, nc, b.w, b.w * (lv == 1 ? rho_b : rho_c), mS, lane)) { buried = true; break; }
             for (int w = lane; w < words; w += 32) W.mask[w] = 0u;
             __syncwarp();
             for (int u = 0; u < n_open; ++u) {
-                const int idU = W.open[side][u];
-                const int kU = idU >> 16, lU = idU & 0xffff;
-                const float thU = (kU + 0.5f) * kPi / Kp;
-                const float phU = 2.f * kPi * (float)lU / (float)lattice_row_len(Kp, thU);
-                float sU, cU;
-                sincosf(thU, &sU, &cU);
-                const int kmin = max(0, (int)ceilf((thU - alpha) * K / kPi - 0.5f) - 1);
-                const int kmax = min(K - 1, (int)floorf((thU + alpha) * K / kPi - 0.5f) + 1);
-                if (lane <= kmax - kmin) {                         // row kmin + lane: samples within alpha of U
-                    const int rk = kmin + lane;
-                    const float2 sc = rsc[r0 + rk];
-                    const int rL = rs[rk + 1] - rs[rk];
-                    const float den = sU * sc.x;
-                    const float rhs = den > 1e-6f ? (ca - cU * sc.y) / den : -2.f;
-                    int l0 = 0, cnt = 0;
-                    if (rhs <= -1.f) { cnt = rL; }
-                    else if (rhs <= 1.f) {
-                        const float dphi = acosf(rhs) + 2.f * kPi / rL;
-                        const int a0 = (int)ceilf((phU - dphi) * rL / (2.f * kPi));
-                        const int a1 = (int)floorf((phU + dphi) * rL / (2.f * kPi));
-                        cnt = a1 - a0 + 1;
-                        if (cnt >= rL) cnt = rL; else { l0 = a0; cnt = max(cnt, 0); }
-                    }
-                    for (int c = 0; c < cnt; ++c) {
-                        int l = (l0 + c) % rL;
-                        if (l < 0) l += rL;
-                        const int idx = rs[rk] + l;
-                        atomicOr(&W.mask[idx >> 5], 1u << (idx & 31));
-                    }
+                const int v = W.open[side][u];
+                const int cnt = g_ico_nnbr[nbr0 + v];
+                if (lane < cnt) {
+                    const int idx = g_ico_nbr[(nbr0 + v) * kIcoNbr + lane];
+                    atomicOr(&W.mask[idx >> 5], 1u << (idx & 31));
                 }
-                __syncwarp();
             }
-            // compact the marked samples into W.cand, in index order
+            __syncwarp();
+            // compact the marked vertices into W.cand, in index order
             int total = 0;
             for (int wb = 0; wb < words; wb += 32) {
                 const int w = wb + lane;
@@ -790,18 +726,9 @@ __global__ void __launch_bounds__(32 * kExposureWarps, 4) k_exposure(BuildDesc* 
                 bool miss = false;
                 int id = 0;
                 if (t < total) {
-                    const int idx = W.cand[t];
-                    int lo_k = 0, hi_k = K - 1;                      // row: last k with rs[k] <= idx
-                    while (lo_k < hi_k) {
-                        const int mid = (lo_k + hi_k + 1) >> 1;
-                        if (rs[mid] <= idx) lo_k = mid; else hi_k = mid - 1;
-                    }
-                    const int l = idx - rs[lo_k], L = rs[lo_k + 1] - rs[lo_k];
-                    const float2 sc = rsc[r0 + lo_k];
-                    float sp, cp;                                    // phi - pi keeps the fast sincos in range
-                    __sincosf(2.f * kPi * (float)l / (float)L - kPi, &sp, &cp);
-                    miss = !in_some_cap(W, nc, -sc.x * cp, -sc.x * sp, sc.y);
-                    id = (lo_k << 16) | l;
+                    id = W.cand[t];
+                    const float4 s = g_ico_dirs[id];
+                    miss = !in_some_cap(W, nc, s.x, s.y, s.z);
                 }
                 const unsigned m = __ballot_sync(full, miss);
                 const int at = n_next + __popc(m & below);
@@ -812,7 +739,7 @@ __global__ void __launch_bounds__(32 * kExposureWarps, 4) k_exposure(BuildDesc* 
             __syncwarp();
             if (exposed) break;
             if (n_next == 0) buried = true;
-            else if (lv == kRefineLevels) exposed = true;
+            else if (lv == 2) exposed = true;
             n_open = n_next;
             side ^= 1;
         }
@@ -835,6 +762,124 @@ __global__ void k_finish_exposure(BuildDesc* descs, int n_scenes) {
 // --------------------------------------------------------------------------
 // Host side
 // --------------------------------------------------------------------------
+namespace {
+
+// Geodesic spheres of the exposure test: the icosahedron subdivided 2, 3 and 4
+// times (162, 642, 2562 vertices; each level's vertices come first in the
+// next), their covering radii and the level A -> B, B -> C neighbour lists.
+struct IcoTables {
+    float4 dirs[kIcoC];
+    uint16_t nbr[(kIcoA + kIcoB) * kIcoNbr];
+    uint8_t nnbr[kIcoA + kIcoB];
+    float rho[3];
+    bool ok = false;
+};
+
+using Vec3 = std::array<double, 3>;
+Vec3 sub3(const Vec3& a, const Vec3& b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
+double dot3(const Vec3& a, const Vec3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+Vec3 cross3(const Vec3& a, const Vec3& b) {
+    return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+Vec3 unit3(const Vec3& a) { double n = std::sqrt(dot3(a, a)); return {a[0] / n, a[1] / n, a[2] / n}; }
+double angle3(const Vec3& a, const Vec3& b) { return std::acos(std::max(-1.0, std::min(1.0, dot3(a, b)))); }
+
+// Largest distance from a point of the sphere to the nearest vertex: over the
+// triangles, the circumradius when the circumcentre lies in the triangle,
+// else half the longest edge.
+double covering_radius(const std::vector<Vec3>& v, const std::vector<std::array<int, 3>>& faces) {
+    double worst = 0.;
+    for (const auto& f : faces) {
+        const Vec3 &A = v[f[0]], &B = v[f[1]], &C = v[f[2]];
+        Vec3 n = unit3(cross3(sub3(B, A), sub3(C, A)));
+        if (dot3(n, A) < 0) n = {-n[0], -n[1], -n[2]};
+        const bool inside = dot3(cross3(A, B), n) >= -1e-15 && dot3(cross3(B, C), n) >= -1e-15 &&
+                            dot3(cross3(C, A), n) >= -1e-15;
+        double r = inside ? angle3(n, A)
+                          : 0.5 * std::max(angle3(A, B), std::max(angle3(B, C), angle3(C, A)));
+        worst = std::max(worst, r);
+    }
+    return worst + 1e-9;
+}
+
+const IcoTables& ico_tables() {
+    static IcoTables T;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const double t = (1. + std::sqrt(5.)) / 2.;
+        const double base[12][3] = {{-1, t, 0}, {1, t, 0}, {-1, -t, 0}, {1, -t, 0}, {0, -1, t}, {0, 1, t},
+                                    {0, -1, -t}, {0, 1, -t}, {t, 0, -1}, {t, 0, 1}, {-t, 0, -1}, {-t, 0, 1}};
+        std::vector<Vec3> v;
+        for (const auto& p : base) v.push_back(unit3({p[0], p[1], p[2]}));
+        std::vector<std::array<int, 3>> f = {{0, 11, 5}, {0, 5, 1}, {0, 1, 7}, {0, 7, 10}, {0, 10, 11}, {1, 5, 9},
+                                             {5, 11, 4}, {11, 10, 2}, {10, 7, 6}, {7, 1, 8}, {3, 9, 4}, {3, 4, 2},
+                                             {3, 2, 6}, {3, 6, 8}, {3, 8, 9}, {4, 9, 5}, {2, 4, 11}, {6, 2, 10},
+                                             {8, 6, 7}, {9, 8, 1}};
+        double rho[3];
+        for (int level = 1; level <= 4; ++level) {
+            std::map<std::pair<int, int>, int> mid;
+            auto midpoint = [&](int a, int b) {
+                auto key = std::make_pair(std::min(a, b), std::max(a, b));
+                auto it = mid.find(key);
+                if (it != mid.end()) return it->second;
+                const Vec3 m = {v[a][0] + v[b][0], v[a][1] + v[b][1], v[a][2] + v[b][2]};
+                v.push_back(unit3(m));
+                mid[key] = (int)v.size() - 1;
+                return (int)v.size() - 1;
+            };
+            std::vector<std::array<int, 3>> next;
+            for (const auto& q : f) {
+                const int ab = midpoint(q[0], q[1]), bc = midpoint(q[1], q[2]), ca = midpoint(q[2], q[0]);
+                next.push_back({q[0], ab, ca});
+                next.push_back({q[1], bc, ab});
+                next.push_back({q[2], ca, bc});
+                next.push_back({ab, bc, ca});
+            }
+            f.swap(next);
+            if (level >= 2) rho[level - 2] = covering_radius(v, f);
+        }
+        if ((int)v.size() != kIcoC) return;
+        for (int i = 0; i < kIcoC; ++i)
+            T.dirs[i] = make_float4((float)v[i][0], (float)v[i][1], (float)v[i][2], 0.f);
+        for (int l = 0; l < 3; ++l) {
+            float r = (float)rho[l];
+            if ((double)r < rho[l]) r = std::nextafter(r, 1.f);
+            T.rho[l] = r;
+        }
+        // level A -> B, B -> C: vertices of the finer level within rho_coarse + rho_fine
+        for (int lv = 0; lv < 2; ++lv) {
+            const int n_from = lv == 0 ? kIcoA : kIcoB, n_to = lv == 0 ? kIcoB : kIcoC, off = lv == 0 ? 0 : kIcoA;
+            const double lim = std::cos(rho[lv] + rho[lv + 1] + 1e-6);
+            for (int u = 0; u < n_from; ++u) {
+                int c = 0;
+                for (int w = 0; w < n_to; ++w) {
+                    if (dot3(v[u], v[w]) < lim) continue;
+                    if (c == kIcoNbr) return;                    // table too narrow: T.ok stays false
+                    T.nbr[(off + u) * kIcoNbr + c++] = (uint16_t)w;
+                }
+                T.nnbr[off + u] = (uint8_t)c;
+            }
+        }
+        T.ok = true;
+    });
+    return T;
+}
+
+int upload_ico_tables(cudaStream_t stream) {
+    const IcoTables& T = ico_tables();
+    if (!T.ok) { set_error("exposure test tables could not be made"); return EHSS_ERR_VALUE; }
+    int rc = cuda_status(cudaMemcpyToSymbolAsync(g_ico_dirs, T.dirs, sizeof(T.dirs), 0, cudaMemcpyHostToDevice, stream),
+                         "exposure table upload");
+    if (!rc) rc = cuda_status(cudaMemcpyToSymbolAsync(g_ico_nbr, T.nbr, sizeof(T.nbr), 0, cudaMemcpyHostToDevice, stream),
+                              "exposure table upload");
+    if (!rc) rc = cuda_status(cudaMemcpyToSymbolAsync(g_ico_nnbr, T.nnbr, sizeof(T.nnbr), 0, cudaMemcpyHostToDevice,
+                                                      stream), "exposure table upload");
+    if (!rc) rc = cuda_status(cudaMemcpyToSymbolAsync(g_ico_rho, T.rho, sizeof(T.rho), 0, cudaMemcpyHostToDevice, stream),
+                              "exposure table upload");
+    return rc;
+}
+
+}  // namespace
 static size_t cub_sort_bytes(int64_t N) {
     size_t bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint64_t*)nullptr, (uint64_t*)nullptr,
@@ -970,6 +1015,8 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
     rc = tree_pass(nullptr);
     if (rc || !exterior) return rc;
     // exterior scenes: mark buried atoms with the full tree, then rebuild over the exposed ones
+    rc = upload_ico_tables(stream);
+    if (rc) return rc;
     {
         int64_t want = (N + kExposureWarps - 1) / kExposureWarps;
         int per_sm = 0;
