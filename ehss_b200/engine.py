@@ -192,10 +192,12 @@ class PreparedStaticGPUEHSS:
     reference's median-split groups, and the GPU replaces worker threads).
     """
 
-    def __init__(self, spheres, groups=None, leaf_size=4, threads=1, boundary='sphere', simplify=False,
+    def __init__(self, spheres, groups=None, leaf_size=None, threads=1, boundary='sphere', simplify=False,
                  coverage_depth=4, precision='fp32', device=None):
+        # leaf_size bounds the device LBVH leaves (capped at 16); left out, the fast default is used
         if type(threads) is not int or threads < 1:
             raise ValueError('Threads must be a positive integer')
+        leaf_size = _lib.DEFAULT_LEAF if leaf_size is None else leaf_size
         if type(leaf_size) is not int or leaf_size < 1:
             raise ValueError('Positive integer leaf size required')
         start = time.perf_counter()
@@ -219,7 +221,8 @@ class PreparedStaticGPUEHSS:
 class SphereIndex:
     """Any-hit PA index (SphereIndex(spheres, kind, leaf_size).query)."""
 
-    def __init__(self, spheres, kind='bvh', leaf_size=4, device=None):
+    def __init__(self, spheres, kind='bvh', leaf_size=None, device=None):
+        leaf_size = _lib.DEFAULT_LEAF if leaf_size is None else leaf_size
         if kind not in ('bvh', 'octree') or leaf_size < 1:
             raise ValueError('Valid kind, positive leaf size and nonempty primitives required.')
         self.spheres = spheres
