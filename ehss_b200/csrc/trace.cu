@@ -705,9 +705,11 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
         const uint32_t flags = B->flags;
         const int64_t ray0 = (c - B->chunk_begin) * (int64_t)chunk_rays;
         const int cnt = (int)min((long long)chunk_rays, (long long)((1ll << B->log2_rays) - ray0));
-        const SceneView S = scene_view(B->scene);
-        const bool ok = S.h->magic == kSceneMagic && S.h->status == 0;
-        const int n_nodes = S.h->n_nodes;
+        // only the scene's base stays live across the phases; each phase rebuilds the view
+        // it needs from the (L1-resident) header, which keeps the traversal's registers free
+        const void* const sbase = B->scene;
+        const bool ok = scene_view(sbase).h->magic == kSceneMagic && scene_view(sbase).h->status == 0;
+        const int n_nodes = scene_view(sbase).h->n_nodes;
         if (lane < kSmemBins) { A.count[lane] = 0; A.ledger[lane] = 0; }
         if (lane == 0) {
             const uint4 b0 = make_uint4(B->base[0], B->base[1], B->base[2], B->base[3]);
@@ -725,6 +727,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
         while (true) {
             // ---- resolve finished queries (FP64) ----
             if (status == kDone) {
+                const SceneView S = scene_view(sbase);
                 int k;
                 double best;
                 if (W.error) {
@@ -786,6 +789,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
             // ---- new rays for lanes whose ray finished ----
             unsigned need = __ballot_sync(0xffffffffu, status == kNeedRay);
             if (need) {
+                const SceneView S = scene_view(sbase);
                 if (status == kNeedRay) {
                     int p = pool + __popc(need & lt_mask);
                     if (p < cnt) {
@@ -830,6 +834,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
             }
             if (!__any_sync(0xffffffffu, status == kTraverse)) break;
             // ---- traverse until enough queries are finished ----
+            const SceneView S = scene_view(sbase);
             while (true) {
                 if (status == kTraverse) {
                     // inner nodes; the first leaf reached is postponed
