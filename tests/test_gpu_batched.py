@@ -80,8 +80,12 @@ def test_exterior_scenes_give_identical_blocks(eb, precision):
     """Buried atoms left out of the trees change no outcome of any block."""
     from ehss_b200.batch import BatchCCS
     from ehss_b200.blocks import DEFAULT_LAUNCH
-    structures = _structures([1, 3, 40, 700, 3000], seed=31) + [_lattice()]
-    seeds = [5, 6, 7, 8, 9, 10]
+    # degenerate cases: duplicated atoms, small atoms nested in large ones, a collinear chain
+    dup = (np.repeat(np.array([[0., 0., 0.], [1.5, 0., 0.], [0., 1.5, 0.]]), 3, axis=0), np.full(9, 1.7))
+    nest = (np.array([[0., 0., 0.], [0.2, 0., 0.], [0., 0.3, 0.1], [2.5, 0., 0.]]), np.array([3.0, 0.8, 1.2, 2.0]))
+    chain = (np.stack([np.arange(30) * 1.1, np.zeros(30), np.zeros(30)], 1), np.full(30, 1.6))
+    structures = _structures([1, 3, 40, 700, 3000], seed=31) + [_lattice(), dup, nest, chain]
+    seeds = [5, 6, 7, 8, 9, 10, 11, 12, 13]
     kw = dict(repeats=2, cap=64, precision=precision, pa=True, graph=False,
               launch=dict(DEFAULT_LAUNCH, count_tests=True))
     full = BatchCCS(structures, 13, seeds, exterior=False, **kw)
@@ -94,7 +98,8 @@ def test_exterior_scenes_give_identical_blocks(eb, precision):
             assert {k: rx[k] for k in keys} == {k: ry[k] for k in keys}
     infos = [ext.batch.info(i) for i in range(len(structures))]
     assert all(i.exterior == 1 and 1 <= i.n_active <= i.n_atoms for i in infos)
-    assert infos[-1].n_active == 216 - 64            # the lattice's 4^3 inner atoms are buried
+    assert infos[5].n_active == 216 - 64             # the lattice's 4^3 inner atoms are buried
+    assert infos[7].n_active == 2                    # the nested atoms are held by the large one
     assert infos[4].n_active < infos[4].n_atoms      # and so are a globule's core atoms
     assert all(full.batch.info(i).n_active == n for i, n in enumerate(full.n_atoms))
     tests = lambda out: sum(r['sphere_tests'] for o in out for r in o['runs'])
