@@ -9,21 +9,27 @@
 // that provably contain no nearer entry.
 //
 // Pipeline (one launch each, all structures of a batch at once):
-//   1. k_stats     per structure: sequential FP64 mean of the centres (the
-//                  order numpy's mean(axis=0) uses), enclosing radius R,
-//                  scale S, largest radius, centre bounds, input validation
+//   1. k_stats     per structure: scene header (layout offsets), sequential
+//                  FP64 mean of the centres (the order numpy's mean(axis=0)
+//                  uses), enclosing radius R, scale S, largest radius, centre
+//                  bounds, input validation
 //   2. k_morton    per atom: 30-bit Morton code of the centre in its
-//                  structure's centre box; key = structure << 30 | code
+//                  structure's centre box; key = structure << 31 | buried << 30
+//                  | code (buried only in the second pass of an exterior build)
 //   3. CUB radix sort of (key, atom) pairs -- stable, so equal codes keep
 //                  atom order
 //   4. k_karras    per internal node: Karras (2012) range / split search
-//                  within the structure's segment
+//                  within the structure's segment of tree atoms
 //   5. k_refit     per atom: FP32 boxes rounded outward, unioned bottom-up
 //                  with one atomic arrival counter per internal node
-//   6. k_emit      per internal node: 64-byte traversal record with both
-//                  child boxes (expanded by eps_box), subtrees of at most
-//                  leaf_size atoms collapsed into leaf references; per atom:
-//                  FP32 and FP64 atom records in leaf order, id maps.
+//   6. k_emit_*    per internal node: 128-byte 4-wide record built from the
+//                  binary node's children and grandchildren (boxes expanded
+//                  by eps_box; subtrees of at most leaf_size atoms collapsed
+//                  into leaf references); per atom: FP32 and FP64 records in
+//                  leaf order, id maps.
+// Exterior builds (EHSS_BUILD_EXTERIOR) then run k_exposure on that tree and
+// repeat steps 2-6 with the buried atoms sorted behind the exposed ones and
+// left out of the tree.
 #include <cub/device/device_radix_sort.cuh>
 #include <algorithm>
 #include <array>

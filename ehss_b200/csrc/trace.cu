@@ -10,8 +10,8 @@
 //
 // Query design.  The reference walks a median-split tree in pre-order and
 // keeps the lexicographic (distance, atom id) minimum of the FP64 entry
-// distances.  Here a binary LBVH is walked near-child-first with a per-thread
-// stack; node boxes are FP32, rounded outward and expanded by eps_box, so a
+// distances.  Here the 4-wide LBVH is walked near-child-first with a
+// per-thread stack; node boxes are FP32, rounded outward and expanded by eps_box, so a
 // box is culled only when it provably holds no entry at or before the
 // current bound U.  Two sphere-test precisions share the walk:
 //   EXACT (EHSS_PREC_FP64): every reached sphere is tested with the
