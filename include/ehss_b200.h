@@ -125,7 +125,7 @@ int ehss_scenes_build(int n_scenes, const double* const* xyz_dev, const double* 
 
 /* Batched build with options.  No counterpart in the reference.
  * EHSS_BUILD_EXTERIOR leaves buried atoms out of the tree: an atom whose
- * whole surface lies inside other atoms (tested on latitude lattices whose
+ * whole surface lies inside other atoms (tested on geodesic sample lattices whose
  * covering radius is added to the required depth) is never the nearest entry
  * of a ray that starts outside the union of the spheres, which every
  * impact-disk ray and every EHSS bounce point does, so the fused block trace
