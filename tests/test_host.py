@@ -211,3 +211,34 @@ def test_block_readout_matches_per_block_formulas():
     words[:n * _RESULT_WORDS] = res.ravel()
     with pytest.raises(_lib.EHSSDeviceError):
         plan.collect()
+
+
+def test_weighted_readout_of_boundary_blocks():
+    """Blocks with caller-made weighted rays report hits, tail and PA from the
+    weighted fixed-point sums; impact-disk blocks from counts (host only)."""
+    import torch
+    from ehss_b200 import _lib
+    from ehss_b200.blocks import BlockJob, BlockPlan, _RESULT_WORDS, _STATS0
+
+    class FakeScene:
+        ptr, radius, device, n_atoms = 0x10000, 5.0, torch.device('cpu'), 10
+
+    jobs = [BlockJob(FakeScene(), 10, 1, cap=4, pa=True, tag=0), BlockJob(FakeScene(), 10, 2, cap=4, pa=True, tag=1)]
+    plan = BlockPlan(jobs, device=torch.device('cpu'))
+    plan._weighted = np.array([False, True])          # block 1 as if its rays carried weights
+    plan._w = np.array([plan._w[0], 0.25])
+    words = plan.packed.numpy().view(np.uint64)
+    res = np.zeros((2, _RESULT_WORDS), dtype=np.uint64)
+    res[:, 0] = 3 << 36                                 # angle sums
+    res[:, 1], res[:, 2], res[:, 4] = 7, 2, 5           # counts
+    res[:, 5], res[:, 6], res[:, 7] = 6 << 35, 1 << 36, 9 << 34   # weighted sums: 3.0, 1.0, 2.25
+    words[:2 * _RESULT_WORDS] = res.ravel()
+    a, b = plan.collect()
+    w0 = plan._w[0]
+    assert a['pa_from_same_rays_angstrom2'] == w0 * 7 and a['tail_bound_angstrom2'] == 2 * w0 * 2
+    assert a['pa_angstrom2'] == w0 * 5 and a['ehss_angstrom2'] == w0 * 3.0
+    assert b['pa_from_same_rays_angstrom2'] == 0.25 * 3.0 and b['tail_bound_angstrom2'] == 2 * 0.25 * 1.0
+    assert b['pa_angstrom2'] == 0.25 * 2.25 and b['ehss_angstrom2'] == 0.25 * 3.0
+    assert b['unresolved_rays'] == 2 and b['collision_histogram'] == [0] * 5
+    t = plan.totals(plan.fetch())
+    assert list(t['tail']) == [2 * w0 * 2, 2 * 0.25 * 1.0] and list(t['pa']) == [w0 * 5, 0.25 * 2.25]
