@@ -335,18 +335,7 @@ class BlockPlan:
             secs = time.perf_counter() - tick
             for r, i in enumerate(need):
                 st = state[i]
-                angle, esc, unres, cont = (int(x) for x in e[r])
-                old = st['cap']
-                st['hist'] += [0] * (new_cap - old)
-                st['ledger'] += [0] * (new_cap - old)
-                st['hist'][old] -= cont
-                for k in range(old, new_cap + 1):
-                    st['hist'][k] += int(ehh[r, k])
-                    st['ledger'][k] += int(ell[r, k])
-                st['angle_fx'] += angle
-                st['escaped'] += esc
-                st['unresolved'] += unres - cont
-                st['cap'] = new_cap
+                cont = merge_extension(st, e[r], ehh[r], ell[r], new_cap)
                 w = float(self._w[i])
                 attempts[i].append(dict(cap=new_cap, ehss_angstrom2=w * (st['angle_fx'] * _lib.FX_SCALE),
                                         tail_bound_angstrom2=2 * w * st['unresolved'],
@@ -363,6 +352,28 @@ class BlockPlan:
             d.update(cap=st['cap'], cap_attempts=attempts[i])
             final.append(d)
         return final
+
+
+def merge_extension(st, ext, hist, ledger, new_cap):
+    """Fold one block's cap extension into its integer totals.  ``st`` holds
+    cap, angle_fx, escaped, unresolved and the hist/ledger lists (cap + 1
+    entries); ``ext`` = (angle_fx, escaped, unresolved, continued) of the
+    continued rays and hist/ledger their rows (new_cap + 1 entries).  The
+    continued rays all stood at bounces == cap, so they leave that bin.
+    Returns the number of continued rays."""
+    angle, esc, unres, cont = (int(x) for x in ext)
+    old = st['cap']
+    st['hist'] += [0] * (new_cap - old)
+    st['ledger'] += [0] * (new_cap - old)
+    st['hist'][old] -= cont
+    for k in range(old, new_cap + 1):
+        st['hist'][k] += int(hist[k])
+        st['ledger'][k] += int(ledger[k])
+    st['angle_fx'] += angle
+    st['escaped'] += esc
+    st['unresolved'] += unres - cont
+    st['cap'] = new_cap
+    return cont
 
 
 def seed_schedule(seed, repeats):

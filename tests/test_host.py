@@ -242,3 +242,18 @@ def test_weighted_readout_of_boundary_blocks():
     assert b['unresolved_rays'] == 2 and b['collision_histogram'] == [0] * 5
     t = plan.totals(plan.fetch())
     assert list(t['tail']) == [2 * w0 * 2, 2 * 0.25 * 1.0] and list(t['pa']) == [w0 * 5, 0.25 * 2.25]
+
+
+def test_cap_extension_merge():
+    """A block at cap 4 with 3 unresolved rays continued to cap 8: two escape
+    (at 5 and 7 bounces), one is still unresolved at 8 (host only)."""
+    from ehss_b200.blocks import merge_extension
+    st = dict(cap=4, angle_fx=100, escaped=10, unresolved=3, hist=[5, 3, 2, 0, 3], ledger=[0, 40, 60, 0, 0])
+    hist = [0] * 9; ledger = [0] * 9
+    hist[5], hist[7], hist[8] = 1, 1, 1
+    ledger[5], ledger[7] = 11, 13
+    cont = merge_extension(st, (24, 2, 1, 3), hist, ledger, 8)
+    assert cont == 3 and st['cap'] == 8
+    assert st['hist'] == [5, 3, 2, 0, 0, 1, 0, 1, 1] and sum(st['hist']) == 13
+    assert st['ledger'] == [0, 40, 60, 0, 0, 11, 0, 13, 0]
+    assert (st['angle_fx'], st['escaped'], st['unresolved']) == (124, 12, 1)
