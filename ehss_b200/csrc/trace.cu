@@ -22,7 +22,7 @@
 //     projections, Edisc on the discriminant).  Certain misses are dropped;
 //     certain hits give an interval [t - Et, t + Et] and lower U to t + Et;
 //     every sphere whose lower bound is <= U (certain or near-tangent) is
-//     kept in a 4-entry candidate list, re-tested in FP64 at the end with the
+//     kept in a 2-entry candidate list, re-tested in FP64 at the end with the
 //     reference formula and the (distance, id) rule.  The reached candidates
 //     always contain the FP64 winner, so outcomes equal EXACT's; a full list
 //     re-runs the query in EXACT mode.
@@ -34,7 +34,13 @@
 namespace ehss {
 
 constexpr float kU32 = 5.9604645e-08f;   // 2^-24
-constexpr int kCand = 4;
+// Candidate slots per query.  A slot whose lower bound exceeds the current U is
+// reused, so two slots overflow only when three spheres are within the error
+// band of each other (89 of 124 M queries on the mixed 256-globule batch).  Each
+// slot is two registers of the fused kernel, which runs at its 64-register
+// bound: 2 slots trace that batch in 27.9 ms, 3 in 28.8, 4 in 29.7, while 1
+// slot sends every grazing query to the FP64 re-run (1e5 fallbacks, 29.0 ms).
+constexpr int kCand = 2;
 constexpr int kSmemBins = 16;
 
 struct LocalStats {
