@@ -112,6 +112,43 @@ class BatchScenes:
                                             self._scenes, self._sizes, self.ws_ptr, self.ws_bytes, self.flags,
                                             stream_handle(self.device)), 'batched scene build')
 
+    def stage(self, structures):
+        """Write new coordinates (and radii) of the same structures into the
+        pinned staging buffers; returns their enclosing radii."""
+        if len(structures) != len(self.scenes):
+            raise ValueError('Refit requires fixed primitive identities.')
+        hx, hr = self.h_xyz.numpy(), self.h_r.numpy()
+        radii = []
+        for (c, r), a0, n in zip(structures, self.atom0, self.n_atoms):
+            c = np.ascontiguousarray(c, dtype=np.float64); r = np.ascontiguousarray(r, dtype=np.float64)
+            if c.shape != (n, 3) or r.shape != (n,):
+                raise ValueError('Refit requires fixed primitive identities.')
+            if not np.isfinite(c).all() or not np.isfinite(r).all() or np.any(r <= 0):
+                raise ValueError('Finite centers (N,3) and positive finite radii required.')
+            radii.append(enclosing_radius(c, r))
+        # an earlier upload from the staging buffers may still be in flight
+        torch().cuda.current_stream(self.device).synchronize()
+        for (c, r), a0, n in zip(structures, self.atom0, self.n_atoms):
+            hx[3 * a0:3 * (a0 + n)] = np.asarray(c, dtype=np.float64).ravel()
+            hr[a0:a0 + n] = r
+        return radii
+
+    def refit(self, structures):
+        """New coordinates of the same structures with every tree's topology
+        kept (ehss_scenes_refit, one pass over the batch): the multi-frame
+        form of SphereIndex.refit (pa_spatial.py:166-170).  Full scenes only;
+        block plans made before a refit keep the old impact-disk radii, so
+        make them after it."""
+        if self.flags & _lib.BUILD_EXTERIOR:
+            raise ValueError('exterior scenes cannot be refit: their trees hold the atoms exposed in the built coordinates')
+        radii = self.stage(structures)
+        self.upload()
+        _lib.check(_lib.load().ehss_scenes_refit(len(self.scenes), self._xyz_ptrs, self._r_ptrs, self._n,
+                                                 self._scenes, self.ws_ptr, self.ws_bytes,
+                                                 stream_handle(self.device)), 'batched scene refit')
+        for sc, R in zip(self.scenes, radii):
+            sc.radius = R
+
     def info(self, i):
         """Header of scene i (synchronises the stream)."""
         info = _lib.SceneInfo()

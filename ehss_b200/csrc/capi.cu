@@ -172,6 +172,18 @@ int ehss_scenes_build_ex(int n_scenes, const double* const* xyz_dev, const doubl
                         workspace_dev, workspace_bytes, as_stream(stream), (flags & EHSS_BUILD_EXTERIOR) != 0);
 }
 
+int ehss_scenes_refit(int n_scenes, const double* const* xyz_dev, const double* const* radii_dev,
+                      const int64_t* n_atoms_host, void* const* scenes_dev, void* workspace_dev,
+                      uint64_t workspace_bytes, void* stream) {
+    clear_error();
+    if (n_scenes < 1 || !xyz_dev || !radii_dev || !n_atoms_host || !scenes_dev || !workspace_dev) {
+        set_error("invalid arguments");
+        return EHSS_ERR_VALUE;
+    }
+    return refit_scenes(n_scenes, xyz_dev, radii_dev, n_atoms_host, scenes_dev, workspace_dev, workspace_bytes,
+                        as_stream(stream));
+}
+
 int ehss_scene_info_get(const void* scene_dev, ehss_scene_info* info, void* stream) {
     clear_error();
     if (!scene_dev || !info) { set_error("null pointer"); return EHSS_ERR_VALUE; }
@@ -182,6 +194,8 @@ int ehss_scene_info_get(const void* scene_dev, ehss_scene_info* info, void* stre
     rc = cuda_status(cudaStreamSynchronize(as_stream(stream)), "scene header read");
     if (rc) return rc;
     if (h.magic != kSceneMagic) { set_error("not a built scene buffer"); return EHSS_ERR_VALUE; }
+    if (h.status == 3) { set_error("refit requires a full (non-exterior) scene with the same atom count"); return EHSS_ERR_VALUE; }
+    if (h.status == 4) { set_error("refit found a malformed node record"); return EHSS_ERR_VALUE; }
     if (h.status != 0) { set_error("scene input has a non-positive or non-finite radius or coordinate"); return EHSS_ERR_VALUE; }
     info->n_atoms = h.n_atoms;
     info->n_nodes = h.n_nodes;

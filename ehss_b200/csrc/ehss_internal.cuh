@@ -235,6 +235,8 @@ uint64_t build_workspace_bytes(int64_t N, int S);
 int build_scenes(int S, const double* const* xyz, const double* const* radii, const int64_t* n, int leaf_size,
                  void* const* scenes, const uint64_t* scene_bytes, void* workspace, uint64_t workspace_bytes,
                  cudaStream_t stream, bool exterior = false);
+int refit_scenes(int S, const double* const* xyz, const double* const* radii, const int64_t* n, void* const* scenes,
+                 void* workspace, uint64_t workspace_bytes, cudaStream_t stream);
 int launch_trace_rays(const void* scene, int64_t n, int cap, int precision, double* P, double* D,
                       const int64_t* last, int64_t* bounces, uint8_t* esc, uint8_t* unres, int32_t* hist,
                       uint64_t* stats, cudaStream_t stream);

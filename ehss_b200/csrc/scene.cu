@@ -54,7 +54,14 @@ struct BuildDesc {
     int32_t exterior;
     int64_t n_active;          // atoms in the tree (exterior scenes: the exposed atoms)
     double cmin[3], cext[3];   // centre box relative to the scene centre (filled by k_stats)
+    int32_t refit;             // 1: new coordinates for an existing full scene (tree kept)
+    int32_t pad;
 };
+
+// Header status codes (0 = valid scene).
+constexpr int32_t kStatusBadInput = 1;     // non-positive or non-finite radius, non-finite coordinate
+constexpr int32_t kStatusRefitMismatch = 3;   // refit of a scene that is not a full scene of n atoms
+constexpr int32_t kStatusCorrupt = 4;      // refit found a malformed node record
 
 struct BuildWork {
     BuildDesc* descs;
@@ -85,12 +92,29 @@ __global__ void k_stats(BuildDesc* descs, int n_scenes) {
     const int64_t n = D.n;
     __shared__ double center[3];
     __shared__ int bad;
-    // header: zeroed, then the layout offsets (the rest is filled below and by k_emit_nodes)
-    if (threadIdx.x < sizeof(SceneHeader) / 4) reinterpret_cast<uint32_t*>(H)[threadIdx.x] = 0u;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        bad = 0;
-        scene_layout(n, &H->off_nodes, &H->off_atoms, &H->off_atoms64, &H->off_ids, &H->off_rank, &H->bytes);
+    if (D.refit) {
+        // refit: the tree fields stay; the scene must be a valid full scene of n atoms
+        __shared__ int mismatch;
+        if (threadIdx.x == 0) {
+            uint64_t on, oa, o64, oi, orr, total;
+            scene_layout(n, &on, &oa, &o64, &oi, &orr, &total);
+            mismatch = !(H->magic == kSceneMagic && H->status == 0 && H->exterior == 0 && H->n_atoms == n &&
+                         H->n_active == n && H->n_nodes >= 1 && H->n_nodes <= (n > 1 ? n - 1 : 1) &&
+                         H->off_nodes == on && H->off_atoms == oa && H->off_atoms64 == o64 && H->off_ids == oi &&
+                         H->off_rank == orr && H->bytes == total);
+            if (mismatch) H->status = kStatusRefitMismatch;
+            bad = 0;
+        }
+        __syncthreads();
+        if (mismatch) return;
+    } else {
+        // header: zeroed, then the layout offsets (the rest is filled below and by k_emit_nodes)
+        if (threadIdx.x < sizeof(SceneHeader) / 4) reinterpret_cast<uint32_t*>(H)[threadIdx.x] = 0u;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            bad = 0;
+            scene_layout(n, &H->off_nodes, &H->off_atoms, &H->off_atoms64, &H->off_ids, &H->off_rank, &H->bytes);
+        }
     }
     __syncthreads();
     // Sequential sum, one lane per coordinate: numpy's mean(axis=0) adds the
@@ -152,9 +176,9 @@ __global__ void k_stats(BuildDesc* descs, int n_scenes) {
     __syncthreads();
     if (threadIdx.x == 0) {
         H->magic = kSceneMagic;
-        H->status = bad ? 1 : 0;
+        H->status = bad ? kStatusBadInput : 0;
         H->n_atoms = (int32_t)n;
-        H->leaf_size = D.leaf_size;
+        if (!D.refit) H->leaf_size = D.leaf_size;
         for (int c = 0; c < 3; ++c) H->center[c] = center[c];
         H->rmax = result[0];
         H->scale = result[1];
@@ -430,6 +454,136 @@ __global__ void k_fill_scene_index(const BuildDesc* descs, int n_scenes, int32_t
     if (s >= n_scenes) return;
     const BuildDesc& D = descs[s];
     for (int64_t i = threadIdx.x; i < D.n; i += blockDim.x) atom_scene[D.atom0 + i] = s;
+}
+
+// --------------------------------------------------------------------------
+// Refit: new coordinates for a full scene, tree topology kept (the reference's
+// SphereIndex.refit / _refit, pa_spatial.py:78-95, 166-170).  k_stats (refit
+// mode) rewrites the header from the new coordinates; then
+//   k_refit_atoms   per leaf-order slot: FP32/FP64 records of the atom it
+//                   holds (ids unchanged) and its outward-rounded box
+//   k_node_links    per 4-wide node: parent link of each node child, count
+//                   of node children
+//   k_refit_nodes   per 4-wide node without node children: child boxes from
+//                   the atom boxes, then up the parent links; the last child
+//                   to finish a node (atomic arrival count) fits the node
+// A node child's slot box is the union of that node's slot boxes before the
+// eps_box expansion, i.e. the union of all its atoms' boxes, which is exactly
+// the box a build with this topology computes.  Node indices of structure s
+// start at descs[s].inner0 (sum of max(n - 1, 1) over the structures before).
+// --------------------------------------------------------------------------
+__device__ __forceinline__ bool refit_live(const BuildDesc& D) {
+    const SceneHeader* H = reinterpret_cast<const SceneHeader*>(D.scene);
+    return D.refit && H->status == 0;
+}
+
+__global__ void k_refit_atoms(const BuildDesc* descs, const int32_t* atom_scene, int64_t N, float* leaf_box) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= N) return;
+    const BuildDesc& D = descs[atom_scene[g]];
+    if (!refit_live(D)) return;
+    SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
+    const int64_t j = g - D.atom0;
+    const int32_t* ids = reinterpret_cast<const int32_t*>(D.scene + H->off_ids);
+    const int64_t a = ids[j];
+    if (a < 0 || a >= D.n) { H->status = kStatusCorrupt; return; }
+    float4* atoms = reinterpret_cast<float4*>(D.scene + H->off_atoms);
+    double4* atoms64 = reinterpret_cast<double4*>(D.scene + H->off_atoms64);
+    double x = D.xyz[a * 3], y = D.xyz[a * 3 + 1], z = D.xyz[a * 3 + 2], r = D.radii[a];
+    atoms[j] = make_float4(__double2float_rn(x - H->center[0]), __double2float_rn(y - H->center[1]),
+                           __double2float_rn(z - H->center[2]), __double2float_rn(r));
+    atoms64[j] = make_double4(x, y, z, r);
+    float b[6];
+    atom_box(D, H, a, b);
+    for (int k = 0; k < 6; ++k) leaf_box[6 * g + k] = b[k];
+}
+
+// Structure owning global node index g (last s with inner0 <= g).
+__device__ __forceinline__ int node_owner(const BuildDesc* descs, int n_scenes, int64_t g) {
+    int lo = 0, hi = n_scenes - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].inner0 <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_node_links(const BuildDesc* descs, int n_scenes, int64_t nodes_total, int32_t* parent,
+                             int32_t* node_children) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= nodes_total) return;
+    const BuildDesc& D = descs[node_owner(descs, n_scenes, g)];
+    if (!refit_live(D)) return;
+    SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
+    const int i = (int)(g - D.inner0), n_nodes = H->n_nodes;
+    if (i >= n_nodes) return;
+    const float4 rf = reinterpret_cast<const float4*>(D.scene + H->off_nodes)[8 * (int64_t)i + 6];
+    const int ref[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z), __float_as_int(rf.w)};
+    int count = 0;
+    for (int c = 0; c < 4; ++c) {
+        if (ref[c] == kEmptyChild) break;                  // used slots form a prefix
+        if (ref[c] < 0) continue;                          // leaf slot
+        if (ref[c] == i || ref[c] >= n_nodes) { H->status = kStatusCorrupt; return; }
+        parent[D.inner0 + ref[c]] = i;
+        ++count;
+    }
+    node_children[g] = count;
+}
+
+__global__ void k_refit_nodes(const BuildDesc* descs, int n_scenes, int64_t nodes_total, const int32_t* parent,
+                              const int32_t* node_children, const float* leaf_box, float* node_box,
+                              uint32_t* arrivals) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= nodes_total) return;
+    const BuildDesc& D = descs[node_owner(descs, n_scenes, g)];
+    if (!refit_live(D)) return;
+    SceneHeader* H = reinterpret_cast<SceneHeader*>(D.scene);
+    const int n_nodes = H->n_nodes;
+    int node = (int)(g - D.inner0);
+    if (node >= n_nodes || node_children[g] != 0) return;   // walks start at nodes whose slots are all leaves
+    float4* nodes = reinterpret_cast<float4*>(D.scene + H->off_nodes);
+    const float eps = H->eps_box;
+    // a walk longer than any tree depth means a malformed link
+    for (int hops = 0; hops < 128; ++hops) {
+        const int64_t gi = D.inner0 + node;
+        const float4 rf = nodes[8 * (int64_t)node + 6];
+        int ref[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z), __float_as_int(rf.w)};
+        float box[4][6];
+        float u[6] = {CUDART_INF_F, CUDART_INF_F, CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F};
+        int used = 0;
+        for (int c = 0; c < 4; ++c) {
+            if (ref[c] == kEmptyChild) break;              // used slots form a prefix
+            float b[6] = {CUDART_INF_F, CUDART_INF_F, CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F};
+            if (ref[c] < 0) {
+                const int code = ~ref[c];
+                const int first = code >> kLeafBits, cnt = (code & (kMaxLeaf - 1)) + 1;
+                if (first + cnt > D.n) { H->status = kStatusCorrupt; return; }
+                for (int a = first; a < first + cnt; ++a)
+                    for (int k = 0; k < 3; ++k) {
+                        b[k] = fminf(b[k], leaf_box[6 * (D.atom0 + a) + k]);
+                        b[3 + k] = fmaxf(b[3 + k], leaf_box[6 * (D.atom0 + a) + 3 + k]);
+                    }
+            } else {
+                if (ref[c] >= n_nodes) { H->status = kStatusCorrupt; return; }
+                const float* src = node_box + 6 * (D.inner0 + ref[c]);
+                for (int k = 0; k < 6; ++k) b[k] = __ldcg(src + k);
+            }
+            for (int k = 0; k < 6; ++k) box[c][k] = b[k];
+            for (int k = 0; k < 3; ++k) { u[k] = fminf(u[k], b[k]); u[3 + k] = fmaxf(u[3 + k], b[3 + k]); }
+            ++used;
+        }
+        if (used == 0) { H->status = kStatusCorrupt; return; }
+        write_node4(nodes, node, box, ref, used, eps);
+        for (int k = 0; k < 6; ++k) node_box[6 * gi + k] = u[k];
+        __threadfence();
+        const int up = parent[gi];
+        if (up < 0) return;                                // the root, or a node no record references
+        const int64_t gu = D.inner0 + up;
+        if (atomicAdd(&arrivals[gu], 1u) + 1u < (uint32_t)node_children[gu]) return;   // siblings still running
+        __threadfence();
+        node = up;
+    }
+    H->status = kStatusCorrupt;
 }
 
 // --------------------------------------------------------------------------
@@ -944,6 +1098,7 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
         D.xyz = xyz[s]; D.radii = radii[s]; D.scene = (char*)scenes[s];
         D.n = n[s]; D.atom0 = N; D.inner0 = I; D.leaf_size = leaf_size; D.exterior = exterior ? 1 : 0;
         D.n_active = n[s];
+        D.refit = 0; D.pad = 0;
         N += n[s];
         I += n[s] - 1;
     }
@@ -1037,6 +1192,70 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
     rc = cuda_status(cudaGetLastError(), "exposure launch");
     if (rc) return rc;
     return tree_pass(W.culled);
+}
+
+int refit_scenes(int S, const double* const* xyz, const double* const* radii, const int64_t* n, void* const* scenes,
+                 void* workspace, uint64_t workspace_bytes, cudaStream_t stream) {
+    if (S < 1) { set_error("at least one structure required"); return EHSS_ERR_VALUE; }
+    int64_t N = 0, nodes_total = 0;
+    std::vector<BuildDesc> host(S);
+    for (int s = 0; s < S; ++s) {
+        if (n[s] < 1 || n[s] > (1 << 27)) {
+            set_error("structure %d: atom count %lld outside 1..2^27", s, (long long)n[s]);
+            return EHSS_ERR_VALUE;
+        }
+        if (((uintptr_t)scenes[s] & 255u) != 0) {
+            set_error("structure %d: scene buffer must be 256-byte aligned", s);
+            return EHSS_ERR_VALUE;
+        }
+        BuildDesc& D = host[s];
+        std::memset(&D, 0, sizeof(D));
+        D.xyz = xyz[s]; D.radii = radii[s]; D.scene = (char*)scenes[s];
+        D.n = n[s]; D.atom0 = N; D.inner0 = nodes_total; D.n_active = n[s];
+        D.refit = 1;
+        N += n[s];
+        nodes_total += n[s] > 1 ? n[s] - 1 : 1;        // node records of a full scene (ehss_scene_bytes layout)
+    }
+    if (N > (int64_t)INT32_MAX) {
+        set_error("a batch holds at most %d atoms, got %lld", INT32_MAX, (long long)N);
+        return EHSS_ERR_VALUE;
+    }
+    uint64_t need = build_workspace_bytes(N, S);
+    if (workspace_bytes < need) {
+        set_error("refit workspace holds %llu bytes, %llu required", (unsigned long long)workspace_bytes,
+                  (unsigned long long)need);
+        return EHSS_ERR_CAPACITY;
+    }
+    // the build workspace's regions, reused: nodes_total <= N, so the per-node arrays fit the inner-node ones
+    char* p = (char*)(((uintptr_t)workspace + 255u) & ~(uintptr_t)255u);
+    const int64_t Ia = N > 0 ? N : 1;
+    BuildDesc* descs = (BuildDesc*)p; p += align256(sizeof(BuildDesc) * (uint64_t)S);
+    int32_t* atom_scene = (int32_t*)p; p += align256(4ull * N);
+    p += 2 * align256(8ull * N) + 2 * align256(4ull * N);           // keys, vals (unused)
+    int32_t* node_children = (int32_t*)p; p += align256(8ull * Ia);
+    p += align256(8ull * Ia);                                       // inner_range (unused)
+    int32_t* parent = (int32_t*)p; p += align256(4ull * Ia);
+    p += align256(4ull * N);                                        // parent_leaf (unused)
+    float* node_box = (float*)p; p += align256(24ull * Ia);
+    float* leaf_box = (float*)p; p += align256(24ull * N);
+    p += align256(4ull * Ia);                                       // inner_height (unused)
+    uint32_t* arrivals = (uint32_t*)p;
+
+    int rc = cuda_status(cudaMemcpyAsync(descs, host.data(), sizeof(BuildDesc) * S, cudaMemcpyHostToDevice, stream),
+                         "refit descriptor upload");
+    if (!rc) rc = cuda_status(cudaMemsetAsync(parent, 0xff, 4ull * nodes_total, stream), "refit parent reset");
+    if (!rc) rc = cuda_status(cudaMemsetAsync(node_children, 0, 4ull * nodes_total, stream), "refit link reset");
+    if (!rc) rc = cuda_status(cudaMemsetAsync(arrivals, 0, 4ull * nodes_total, stream), "refit arrival reset");
+    if (rc) return rc;
+    const int T = 256;
+    auto blocks = [&](int64_t count) { return (unsigned)((count + T - 1) / T); };
+    k_fill_scene_index<<<S, 256, 0, stream>>>(descs, S, atom_scene);
+    k_stats<<<S, 256, 0, stream>>>(descs, S);
+    k_refit_atoms<<<blocks(N), T, 0, stream>>>(descs, atom_scene, N, leaf_box);
+    k_node_links<<<blocks(nodes_total), T, 0, stream>>>(descs, S, nodes_total, parent, node_children);
+    k_refit_nodes<<<blocks(nodes_total), T, 0, stream>>>(descs, S, nodes_total, parent, node_children, leaf_box,
+                                                         node_box, arrivals);
+    return cuda_status(cudaGetLastError(), "refit launch");
 }
 
 }  // namespace ehss

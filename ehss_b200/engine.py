@@ -59,6 +59,7 @@ class Scene:
         if c.ndim != 2 or c.shape[1] != 3 or r.shape != (len(c),) or len(c) == 0:
             raise ValueError('Expected nonempty centers (N,3) and radii (N,).')
         self.n_atoms = len(r)
+        self._radii = r.copy()
         self.leaf_size = int(leaf_size)
         sb, wb = ct.c_uint64(), ct.c_uint64()
         _lib.check(lib.ehss_scene_bytes(self.n_atoms, self.leaf_size, ct.byref(sb), ct.byref(wb)), 'scene size')
@@ -77,14 +78,45 @@ class Scene:
         else:
             _lib.check(lib.ehss_scene_build(self.n_atoms, xyz_d.data_ptr(), r_d.data_ptr(), self.leaf_size, self.ptr,
                                             sb.value, ws_addr, wb.value, stream), 'scene build')
-        info = _lib.SceneInfo()
-        _lib.check(lib.ehss_scene_info_get(self.ptr, ct.byref(info), stream), 'scene build')   # synchronises
+        self._read_info('scene build')   # synchronises
         del ws, xyz_d, r_d
+
+    def _read_info(self, what):
+        info = _lib.SceneInfo()
+        _lib.check(_lib.load().ehss_scene_info_get(self.ptr, ct.byref(info), stream_handle(self.device)), what)
         self.info = info
         self.exterior = bool(info.exterior)
         self.n_active = int(info.n_active)
         self.center = np.array(info.center[:])
         self.radius = float(info.radius)
+
+    def refit(self, centers, radii=None):
+        """New coordinates (and optionally radii) for the same atoms, tree
+        topology kept (ehss_scenes_refit; SphereIndex.refit, pa_spatial.py:166-170).
+        The header and atom records become those of a build of the new
+        coordinates and every node box the union of its atoms' boxes, so
+        traces return what a rebuilt scene returns.  Full scenes only."""
+        if self.exterior:
+            raise ValueError('an exterior scene cannot be refit: its tree holds the atoms exposed in the built coordinates')
+        c = np.ascontiguousarray(centers, dtype=np.float64)
+        r = self._radii if radii is None else np.ascontiguousarray(radii, dtype=np.float64)
+        if c.shape != (self.n_atoms, 3) or r.shape != (self.n_atoms,):
+            raise ValueError('Refit requires fixed primitive identities.')
+        if not np.isfinite(c).all() or not np.isfinite(r).all() or np.any(r <= 0):
+            raise ValueError('Finite centers (N,3) and positive finite radii required.')
+        lib = _lib.load()
+        sb, wb = ct.c_uint64(), ct.c_uint64()
+        _lib.check(lib.ehss_scene_bytes(self.n_atoms, self.leaf_size, ct.byref(sb), ct.byref(wb)), 'scene size')
+        xyz_d = to_device(c, np.float64, self.device)
+        r_d = to_device(r, np.float64, self.device)
+        ws, ws_addr = _aligned_buffer(wb.value, self.device)
+        _lib.check(lib.ehss_scenes_refit(1, (ct.c_void_p * 1)(xyz_d.data_ptr()), (ct.c_void_p * 1)(r_d.data_ptr()),
+                                         (ct.c_int64 * 1)(self.n_atoms), (ct.c_void_p * 1)(self.ptr), ws_addr,
+                                         wb.value, stream_handle(self.device)), 'scene refit')
+        self._read_info('scene refit')   # synchronises
+        del ws, xyz_d, r_d
+        self._radii = r.copy()
+        return self
 
     @classmethod
     def from_spheres(cls, spheres, leaf_size=_lib.DEFAULT_LEAF, device=None):
@@ -227,6 +259,14 @@ class SphereIndex:
             raise ValueError('Valid kind, positive leaf size and nonempty primitives required.')
         self.spheres = spheres
         self.scene = Scene.from_spheres(spheres, leaf_size=min(int(leaf_size), 16), device=device)
+
+    def refit(self, spheres):
+        """Same atoms at new positions (SphereIndex.refit, pa_spatial.py:166-170):
+        the device tree is refit in place (ehss_scenes_refit)."""
+        if len(spheres.radii) != len(self.spheres.radii):
+            raise ValueError('Refit requires fixed primitive identities.')
+        self.scene.refit(spheres.centers, spheres.radii)
+        self.spheres = spheres
 
     def query(self, source):
         owners = getattr(source, 'owners', None)

@@ -139,9 +139,28 @@ int ehss_scenes_build_ex(int n_scenes, const double* const* xyz_dev, const doubl
                          const uint64_t* scene_bytes_host, void* workspace_dev, uint64_t workspace_bytes,
                          uint32_t flags, void* stream);
 
+/* Refit: new coordinates (and radii) for scenes built without
+ * EHSS_BUILD_EXTERIOR, same atom count and identities, tree topology kept.
+ * Replaces SphereIndex.refit (pa_spatial.py:166-170, which raises
+ * ValueError('Refit requires fixed primitive identities.') for another atom
+ * count) and the bottom-up box refit (_refit, pa_spatial.py:78-95;
+ * parents, ehss_cpu_geometry.py:58-71).  The header (centre, R, S, rmax,
+ * eps_box) and the FP32/FP64 atom records are recomputed exactly as a build
+ * of the new coordinates computes them; every node box becomes the outward-
+ * rounded union of its atoms' boxes under the old topology, so traversals
+ * return the same (distance, id) choices as on a rebuilt scene (the tree may
+ * be looser after large moves).  Same workspace as ehss_scenes_build.
+ * Asynchronous like the build: a scene that is not a full scene of n_atoms
+ * atoms, or new inputs with a non-positive or non-finite radius or a
+ * non-finite coordinate, leave the scene invalid, reported by
+ * ehss_scene_info_get. */
+int ehss_scenes_refit(int n_scenes, const double* const* xyz_dev, const double* const* radii_dev,
+                      const int64_t* n_atoms_host, void* const* scenes_dev, void* workspace_dev,
+                      uint64_t workspace_bytes, void* stream);
+
 /* Copy the scene header to the host (synchronises `stream`).  Fails with
  * EHSS_ERR_VALUE when the build found a non-positive or non-finite radius or
- * a non-finite coordinate. */
+ * a non-finite coordinate, or a refit found a scene it cannot refit. */
 int ehss_scene_info_get(const void* scene_dev, ehss_scene_info* info_host, void* stream);
 
 /* ------------------------------------------------------------------------ */
