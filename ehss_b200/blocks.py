@@ -31,6 +31,18 @@ DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=8, chunk_rays=0, resolve_ba
                       count_tests=False)
 
 
+_SM_COUNT = {}
+
+
+def _sm_count(device):
+    """Multiprocessors of ``device`` (cached: the served form makes a plan per round)."""
+    t = torch()
+    key = t.device(device).index
+    if key not in _SM_COUNT:
+        _SM_COUNT[key] = t.cuda.get_device_properties(device).multi_processor_count if t.cuda.is_available() else 148
+    return _SM_COUNT[key]
+
+
 def auto_chunk(rays, launch, sm_count):
     """Rays per work item: 256 when every warp of the persistent grid gets
     several chunks (large batches), smaller for small jobs so that a single
@@ -75,8 +87,7 @@ class BlockPlan:
         L = dict(DEFAULT_LAUNCH)
         L.update(launch or {})
         if not L['chunk_rays']:
-            sms = t.cuda.get_device_properties(self.device).multi_processor_count if t.cuda.is_available() else 148
-            L['chunk_rays'] = auto_chunk(sum(1 << j.log2_rays for j in self.jobs), L, sms)
+            L['chunk_rays'] = auto_chunk(sum(1 << j.log2_rays for j in self.jobs), L, _sm_count(self.device))
         precisions = 0
         for j in jobs:
             precisions |= 1 << int(j.precision)
@@ -119,8 +130,11 @@ class BlockPlan:
         _lib.check(lib.ehss_blocks_prepare(host, n, seeds, self.launch.chunk_rays, ct.byref(total)), 'blocks')
         self.total_chunks = total.value
         self.hist_entries = offset
-        raw = np.frombuffer(bytes(host), dtype=np.uint8)
-        self.blocks_dev = t.from_numpy(raw.copy()).to(self.device)
+        # descriptors through pinned memory: the upload does not wait for earlier work on the stream
+        self._blocks_host = t.empty(ct.sizeof(host), dtype=t.uint8,
+                                    pin_memory=t.device(self.device).type == 'cuda')
+        ct.memmove(self._blocks_host.data_ptr(), ct.addressof(host), ct.sizeof(host))
+        self.blocks_dev = self._blocks_host.to(self.device, non_blocking=True)
         # block totals, histograms and ledgers in one buffer: one copy back to the host
         H = max(offset, 1)
         nw = n * _RESULT_WORDS

@@ -1025,17 +1025,31 @@ const IcoTables& ico_tables() {
     return T;
 }
 
+// Once per device and process: a copy from pageable memory waits for the
+// stream to drain, which in the middle of a build would leave the GPU idle
+// while the host issues the rest of the build.  The first upload completes
+// before any build proceeds, so builds on other streams see the tables.
 int upload_ico_tables(cudaStream_t stream) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static bool uploaded[kMaxDevices] = {};
+    int dev = -1;
+    int rc = cuda_status(cudaGetDevice(&dev), "exposure table upload");
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < kMaxDevices && uploaded[dev]) return EHSS_OK;
     const IcoTables& T = ico_tables();
     if (!T.ok) { set_error("exposure test tables could not be made"); return EHSS_ERR_VALUE; }
-    int rc = cuda_status(cudaMemcpyToSymbolAsync(g_ico_dirs, T.dirs, sizeof(T.dirs), 0, cudaMemcpyHostToDevice, stream),
-                         "exposure table upload");
+    rc = cuda_status(cudaMemcpyToSymbolAsync(g_ico_dirs, T.dirs, sizeof(T.dirs), 0, cudaMemcpyHostToDevice, stream),
+                     "exposure table upload");
     if (!rc) rc = cuda_status(cudaMemcpyToSymbolAsync(g_ico_nbr, T.nbr, sizeof(T.nbr), 0, cudaMemcpyHostToDevice, stream),
                               "exposure table upload");
     if (!rc) rc = cuda_status(cudaMemcpyToSymbolAsync(g_ico_nnbr, T.nnbr, sizeof(T.nnbr), 0, cudaMemcpyHostToDevice,
                                                       stream), "exposure table upload");
     if (!rc) rc = cuda_status(cudaMemcpyToSymbolAsync(g_ico_rho, T.rho, sizeof(T.rho), 0, cudaMemcpyHostToDevice, stream),
                               "exposure table upload");
+    if (!rc) rc = cuda_status(cudaStreamSynchronize(stream), "exposure table upload");
+    if (!rc && dev >= 0 && dev < kMaxDevices) uploaded[dev] = true;
     return rc;
 }
 
@@ -1180,10 +1194,12 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
     if (rc) return rc;
     {
         int64_t want = (N + kExposureWarps - 1) / kExposureWarps;
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exposure, 32 * kExposureWarps, 0) != cudaSuccess ||
-            per_sm < 1)
-            per_sm = 1;
+        static const int per_sm = [] {
+            int b = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_exposure, 32 * kExposureWarps, 0) != cudaSuccess || b < 1)
+                b = 1;
+            return b;
+        }();
         int64_t cap = (int64_t)per_sm * sm_count();
         unsigned grid = (unsigned)(want < cap ? want : cap);
         k_exposure<<<grid, 32 * kExposureWarps, 0, stream>>>(W.descs, W.atom_scene, N, W.culled);

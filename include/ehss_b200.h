@@ -132,7 +132,8 @@ int ehss_scenes_build(int n_scenes, const double* const* xyz_dev, const double* 
  * (ehss_trace_blocks) gives the same outcomes on an exterior scene with fewer
  * tests.  ehss_trace and ehss_pa_anyhit take arbitrary rays and report every
  * ray of an exterior scene as an error (EHSS_STAT_ERRORS).  flags = 0 is
- * ehss_scenes_build. */
+ * ehss_scenes_build.  The first exterior build on a device uploads the
+ * sample lattices and synchronises `stream`: make it outside stream capture. */
 #define EHSS_BUILD_EXTERIOR 1u
 int ehss_scenes_build_ex(int n_scenes, const double* const* xyz_dev, const double* const* radii_dev,
                          const int64_t* n_atoms_host, int leaf_size, void* const* scenes_dev,
