@@ -80,6 +80,7 @@ _SIGNATURES = {
     'ehss_scenes_workspace_bytes': (ct.c_int, [ct.c_int, P, P]),
     'ehss_scenes_build': (ct.c_int, [ct.c_int, P, P, P, ct.c_int, P, P, P, U64, P]),
     'ehss_scenes_build_ex': (ct.c_int, [ct.c_int, P, P, P, ct.c_int, P, P, P, U64, ct.c_uint32, P]),
+    'ehss_enclosing_radius': (ct.c_int, [I64, P, P, P]),
     'ehss_scenes_refit': (ct.c_int, [ct.c_int, P, P, P, P, P, U64, P]),
     'ehss_scene_info_get': (ct.c_int, [P, P, P]),
     'ehss_source_rays': (ct.c_int, [P, ct.c_int, U64, I64, I64, P, P, P]),

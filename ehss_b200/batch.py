@@ -22,9 +22,13 @@ from .device import require_cuda, stream_handle, torch
 
 
 def enclosing_radius(centers, radii):
-    """Impact-disk radius exactly as the device computes it (ehss_state.py:46-47)."""
-    center = centers.mean(axis=0)
-    return float(np.max(np.linalg.norm(centers - center, axis=1) + radii)) * (1. + 1e-9)
+    """Impact-disk radius exactly as the device computes it (ehss_state.py:46-47;
+    ehss_enclosing_radius, host code)."""
+    c = np.ascontiguousarray(centers, dtype=np.float64)
+    r = np.ascontiguousarray(radii, dtype=np.float64)
+    out = ct.c_double()
+    _lib.check(_lib.load().ehss_enclosing_radius(len(r), c.ctypes.data, r.ctypes.data, ct.byref(out)), 'radius')
+    return out.value
 
 
 def summarize(values):

@@ -109,6 +109,32 @@ int ehss_compact_source_rays(const ehss_boundary* boundary_host, int log2n, uint
                                weights_dev, as_stream(stream));
 }
 
+int ehss_enclosing_radius(int64_t n_atoms, const double* xyz, const double* radii, double* radius) {
+    clear_error();
+    if (n_atoms < 1 || !xyz || !radii || !radius) { set_error("invalid arguments"); return EHSS_ERR_VALUE; }
+    // k_stats' operations: sequential column sums divided by n, then max of |c - centre| + r
+    // (norm as sqrt((x*x + y*y) + z*z)), times 1.000000001; each operation rounded once
+    volatile double acc[3] = {0., 0., 0.};
+    for (int64_t i = 0; i < n_atoms; ++i)
+        for (int c = 0; c < 3; ++c) acc[c] = acc[c] + xyz[3 * i + c];
+    double center[3];
+    for (int c = 0; c < 3; ++c) center[c] = acc[c] / (double)n_atoms;
+    double smax = 0.;
+    bool nan = false;
+    for (int64_t i = 0; i < n_atoms; ++i) {
+        volatile double x = xyz[3 * i] - center[0], y = xyz[3 * i + 1] - center[1], z = xyz[3 * i + 2] - center[2];
+        volatile double xx = x * x, yy = y * y, zz = z * z;
+        volatile double s = xx + yy;
+        s = s + zz;
+        volatile double len = std::sqrt((double)s);
+        len = len + radii[i];
+        if (std::isnan((double)len)) nan = true;
+        else if (len > smax) smax = len;
+    }
+    *radius = nan ? NAN : smax * 1.000000001;
+    return EHSS_OK;
+}
+
 int ehss_scene_bytes(int64_t n_atoms, int leaf_size, uint64_t* scene_bytes, uint64_t* workspace_bytes) {
     clear_error();
     if (n_atoms < 1 || n_atoms > (1 << 27)) {

@@ -141,24 +141,28 @@ bool sobol_scramble(int dim, uint64_t seed, uint32_t* sv, uint32_t* shift) {
         for (int k = 0; k < kBits; ++k) s |= rng.bit() << k;
         shift[j] = s;
     }
-    // L[j][i][l], i = row (output digit, MSB-first), l = column; tril + unit diagonal
-    static thread_local uint8_t L[kMaxDim][kBits][kBits];
+    // Row i of dimension j's matrix (output digit i, MSB-first; tril + unit
+    // diagonal) as a mask over the input word: column l <-> bit 29 - l, so
+    // digit i of the product is the parity of (row & input).  Every bit is
+    // drawn, in numpy's order, including those above the diagonal.
+    uint32_t rows[kMaxDim][kBits];
     for (int j = 0; j < dim; ++j)
-        for (int i = 0; i < kBits; ++i)
+        for (int i = 0; i < kBits; ++i) {
+            uint32_t m = 0;
             for (int l = 0; l < kBits; ++l) {
-                uint8_t b = (uint8_t)rng.bit();
-                L[j][i][l] = (l < i) ? b : (l == i ? 1 : 0);
+                uint32_t b = rng.bit();
+                if (l < i) m |= b << (kBits - 1 - l);
             }
+            rows[j][i] = m | (1u << (kBits - 1 - i));
+        }
     uint32_t v[kMaxDim * kBits];
     sobol_direction_numbers(dim, v);
     for (int j = 0; j < dim; ++j)
         for (int k = 0; k < kBits; ++k) {
-            uint32_t in = v[j * kBits + k], out = 0;
-            for (int i = 0; i < kBits; ++i) {
-                uint32_t acc = 0;
-                for (int l = 0; l <= i; ++l) acc ^= L[j][i][l] & ((in >> (kBits - 1 - l)) & 1u);
-                out |= acc << (kBits - 1 - i);
-            }
+            const uint32_t in = v[j * kBits + k];
+            uint32_t out = 0;
+            for (int i = 0; i < kBits; ++i)
+                out |= (uint32_t)(__builtin_popcount(rows[j][i] & in) & 1) << (kBits - 1 - i);
             sv[j * kBits + k] = out;
         }
     return true;

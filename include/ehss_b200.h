@@ -88,6 +88,13 @@ typedef struct ehss_scene_info {
     int32_t reserved;
 } ehss_scene_info;
 
+/* Impact-disk radius R = max_i(|c_i - mean(c)| + r_i) * (1 + 1e-9) of host
+ * arrays xyz_host[n*3], radii_host[n], computed with the operations and order
+ * of the device builder (and of external_source, ehss_state.py:46-47), so a
+ * caller can weight block results (pi R^2 / n per ray) without reading the
+ * scene header back.  Host only. */
+int ehss_enclosing_radius(int64_t n_atoms, const double* xyz_host, const double* radii_host, double* radius);
+
 /* Bytes of the scene buffer and of the build workspace for n_atoms. */
 int ehss_scene_bytes(int64_t n_atoms, int leaf_size, uint64_t* scene_bytes, uint64_t* workspace_bytes);
 

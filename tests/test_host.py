@@ -257,3 +257,20 @@ def test_cap_extension_merge():
     assert st['hist'] == [5, 3, 2, 0, 0, 1, 0, 1, 1] and sum(st['hist']) == 13
     assert st['ledger'] == [0, 40, 60, 0, 0, 11, 0, 13, 0]
     assert (st['angle_fx'], st['escaped'], st['unresolved']) == (124, 12, 1)
+
+
+def test_enclosing_radius_matches_the_reference_formula(lib):
+    """ehss_enclosing_radius (host) equals external_source's R = max(|c - mean| + r) * (1 + 1e-9)
+    (ehss_state.py:46-47, numpy operation order) bit for bit."""
+    from ehss_b200 import _lib
+    from ehss_b200.batch import enclosing_radius
+    for s in range(200):
+        rng = np.random.default_rng(s)
+        n = int(rng.integers(1, 2000))
+        c = rng.normal(0, 10 ** rng.uniform(-2, 3), (n, 3)) + rng.normal(0, 10 ** rng.uniform(-2, 4), 3)
+        r = rng.uniform(0.5, 3, n)
+        center = c.mean(axis=0)
+        ref = float(np.max(np.linalg.norm(c - center, axis=1) + r)) * (1. + 1e-9)
+        assert enclosing_radius(c, r) == ref
+    out = ct.c_double()
+    assert lib.ehss_enclosing_radius(0, None, None, ct.byref(out)) == _lib.ERR_VALUE
