@@ -146,7 +146,11 @@ __device__ __noinline__ int nearest_flat(const SceneView& S, const double* o, co
 }
 
 // Nearest entry: returns the leaf-order rank of the collider (or -1) and its
-// FP64 entry distance, identical to the reference's choice.
+// FP64 entry distance, identical to the reference's choice.  The explicit-ray
+// kernels and the fused kernel's overflow fallback use it; it restates the
+// Walker's FP32 filter in a self-contained form because the fused kernel's
+// local-memory frame includes this function's, and a Walker-based version
+// (with a LaneRay copy) measured 0.9 % slower on the batched trace.
 template <bool EXACT>
 __device__ __noinline__ int nearest(const SceneView& S, const double* o, const double* d, int last_rank,
                                     double& best_out, LocalStats& st) {
