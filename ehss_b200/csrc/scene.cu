@@ -16,8 +16,10 @@
 //   2. k_morton    per atom: 30-bit Morton code of the centre in its
 //                  structure's centre box; key = structure << 31 | buried << 30
 //                  | code (buried only in the second pass of an exterior build)
-//   3. CUB radix sort of (key, atom) pairs -- stable, so equal codes keep
-//                  atom order
+//   3. stable sort of (key, atom) pairs, so equal codes keep atom order:
+//                  per structure in one CTA (k_morton_segsort, steps 2-3 in one
+//                  launch) when every structure holds at most 8192 atoms, else
+//                  CUB's device-wide radix sort
 //   4. k_karras    per internal node: Karras (2012) range / split search
 //                  within the structure's segment of tree atoms
 //   5. k_refit     per atom: FP32 boxes rounded outward, unioned bottom-up
@@ -30,6 +32,7 @@
 // Exterior builds (EHSS_BUILD_EXTERIOR) then run k_exposure on that tree and
 // repeat steps 2-6 with the buried atoms sorted behind the exposed ones and
 // left out of the tree.
+#include <cub/block/block_radix_sort.cuh>
 #include <cub/device/device_radix_sort.cuh>
 #include <algorithm>
 #include <array>
@@ -205,14 +208,9 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
     return v;
 }
 
-__global__ void k_morton(const BuildDesc* descs, const int32_t* atom_scene, int64_t N, const uint8_t* culled,
-                         uint64_t* keys, int32_t* vals) {
-    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (g >= N) return;
-    int s = atom_scene[g];
-    const BuildDesc& D = descs[s];
-    const SceneHeader* H = reinterpret_cast<const SceneHeader*>(D.scene);
-    int64_t i = g - D.atom0;
+// Morton key of atom i of structure D (low 31 bits: buried flag << 30 | 30-bit
+// code of the centre in the structure's centre box).
+__device__ __forceinline__ uint32_t morton_key31(const BuildDesc& D, const SceneHeader* H, int64_t i, bool buried) {
     uint32_t q[3];
     for (int c = 0; c < 3; ++c) {
         double rel = (D.xyz[i * 3 + c] - H->center[c]) - D.cmin[c];
@@ -222,10 +220,59 @@ __global__ void k_morton(const BuildDesc* descs, const int32_t* atom_scene, int6
         q[c] = (uint32_t)fmin(u * 1024.0, 1023.0);
     }
     uint32_t code = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+    return (buried ? (1u << 30) : 0u) | code;
+}
+
+__global__ void k_morton(const BuildDesc* descs, const int32_t* atom_scene, int64_t N, const uint8_t* culled,
+                         uint64_t* keys, int32_t* vals) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= N) return;
+    int s = atom_scene[g];
+    const BuildDesc& D = descs[s];
+    const SceneHeader* H = reinterpret_cast<const SceneHeader*>(D.scene);
+    int64_t i = g - D.atom0;
     // buried atoms of an exterior build sort after every exposed atom of their structure
-    uint64_t out = culled && D.exterior && culled[g] ? (1ull << 30) : 0ull;
-    keys[g] = ((uint64_t)s << 31) | out | code;
+    const bool buried = culled && D.exterior && culled[g];
+    keys[g] = ((uint64_t)s << 31) | morton_key31(D, H, i, buried);
     vals[g] = (int32_t)i;
+}
+
+// Batches whose structures all hold at most kSegSortMax atoms: keys made and
+// sorted per structure by one CTA (stable block radix sort in shared memory),
+// one launch instead of the device-wide sort's several.  Keys never cross
+// structures, so the result equals the device-wide stable sort of k_morton's
+// keys element for element.  Two sizes: 256 x 8 keys (structures of at most
+// 2048 atoms) and 512 x 16 (8192).
+constexpr int kSegSortMax = 8192, kSegSortSmall = 2048;
+
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_morton_segsort(const BuildDesc* descs,
+                                                                          const uint8_t* culled,
+                                                                          uint64_t* keys_out, int32_t* vals_out) {
+    using SegSort = cub::BlockRadixSort<uint32_t, THREADS, ITEMS, int32_t>;
+    static_assert(sizeof(typename SegSort::TempStorage) <= 48 * 1024, "segment sort storage fits static shared memory");
+    __shared__ typename SegSort::TempStorage temp;
+    const int s = blockIdx.x;
+    const BuildDesc& D = descs[s];
+    const SceneHeader* H = reinterpret_cast<const SceneHeader*>(D.scene);
+    const int n = D.n < THREADS * ITEMS ? (int)D.n : THREADS * ITEMS;     // the host sends no larger structure
+    uint32_t key[ITEMS];
+    int32_t val[ITEMS];
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+        const int i = threadIdx.x * ITEMS + k;              // blocked: item order = atom order
+        val[k] = i;
+        key[k] = i < n ? morton_key31(D, H, i, culled && D.exterior && culled[D.atom0 + i]) : 0xffffffffu;
+    }
+    SegSort(temp).Sort(key, val, 0, 32);
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+        const int j = threadIdx.x * ITEMS + k;
+        if (j < n) {
+            keys_out[D.atom0 + j] = ((uint64_t)s << 31) | key[k];
+            vals_out[D.atom0 + j] = val[k];
+        }
+    }
 }
 
 // Karras (2012), "Maximizing parallelism in the construction of BVHs,
@@ -1087,7 +1134,7 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
                  cudaStream_t stream, bool exterior) {
     if (S < 1) { set_error("at least one structure required"); return EHSS_ERR_VALUE; }
     if (leaf_size < 1 || leaf_size > kMaxLeaf) { set_error("leaf_size must be 1..%d", kMaxLeaf); return EHSS_ERR_VALUE; }
-    int64_t N = 0, I = 0;
+    int64_t N = 0, I = 0, max_n = 0;
     BuildDesc* host = new BuildDesc[S];
     for (int s = 0; s < S; ++s) {
         if (n[s] < 1 || n[s] > (1 << 27)) {
@@ -1113,6 +1160,7 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
         D.n = n[s]; D.atom0 = N; D.inner0 = I; D.leaf_size = leaf_size; D.exterior = exterior ? 1 : 0;
         D.n_active = n[s];
         D.refit = 0; D.pad = 0;
+        if (n[s] > max_n) max_n = n[s];
         N += n[s];
         I += n[s] - 1;
     }
@@ -1163,12 +1211,22 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
     k_stats<<<S, 256, 0, stream>>>(W.descs, S);
     int end_bit = 31;
     while ((1ll << (end_bit - 31)) < S) ++end_bit;
+    const bool segsort = max_n <= kSegSortMax;
     // one pass: Morton keys -> sort -> Karras hierarchy -> refit -> node and atom records
     auto tree_pass = [&](const uint8_t* culled) -> int {
-        k_morton<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, culled, W.keys_in, W.vals_in);
-        size_t cub_bytes = W.cub_bytes;
-        int r = cuda_status(cub::DeviceRadixSort::SortPairs(W.cub_temp, cub_bytes, W.keys_in, W.keys_out, W.vals_in,
+        int r;
+        if (segsort) {
+            if (max_n <= kSegSortSmall)
+                k_morton_segsort<256, 8><<<S, 256, 0, stream>>>(W.descs, culled, W.keys_out, W.vals_out);
+            else
+                k_morton_segsort<512, 16><<<S, 512, 0, stream>>>(W.descs, culled, W.keys_out, W.vals_out);
+            r = cuda_status(cudaGetLastError(), "LBVH key sort");
+        } else {
+            k_morton<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, culled, W.keys_in, W.vals_in);
+            size_t cub_bytes = W.cub_bytes;
+            r = cuda_status(cub::DeviceRadixSort::SortPairs(W.cub_temp, cub_bytes, W.keys_in, W.keys_out, W.vals_in,
                                                             W.vals_out, (int)N, 0, end_bit, stream), "LBVH key sort");
+        }
         if (r) return r;
         // parent links start at -1 so that a missing link ends a refit walk
         r = cuda_status(cudaMemsetAsync(W.parent_leaf, 0xff, 4ull * N, stream), "LBVH parent reset");
