@@ -219,6 +219,7 @@ def serving_measurement(duration_s=2.0, rate=200.0, seed=7):
     reqs = W.request_stream(int(duration_s * rate), rate=rate, seed=seed)
     base, base_r, _ = W.globule(1500, 4242)
     ex = DeviceExecutor()
+    ex.warmup()         # every builder path's kernels loaded before traffic
     # warm-up (context, module, allocator) outside the measurement
     warm = CCSServer(ex, block_log2=15, target=0.01)
     warm.submit(CCSRequest('w', base, base_r, seed=1))

@@ -153,7 +153,11 @@ class CCSServer:
                 nxt = min(s.req.arrival for s in self.pending)
                 wait = nxt - self.now()
                 if wait > 0:
-                    time.sleep(min(wait, 0.05))
+                    # sleep until about 1 ms before the next arrival, then poll: a sleep
+                    # overshoots by up to a scheduler tick, which would land in that
+                    # request's latency
+                    if wait > 2e-3:
+                        time.sleep(min(wait - 1e-3, 0.05))
                     if self.now() - start > timeout_s:
                         raise TimeoutError('serving did not finish in time')
                     continue
@@ -178,6 +182,18 @@ class DeviceExecutor:
         self.leaf_size = _lib.DEFAULT_LEAF if leaf_size is None else int(leaf_size)
         self.cap, self.launch = cap, launch
         self.precision = {'fp64': _lib.PREC_FP64, 'fp32': _lib.PREC_FP32}[precision]
+
+    def warmup(self, sizes=(64, 4096, 12000)):
+        """Build and trace one synthetic structure per builder path (per-structure
+        key sorts of up to 2048 and 8192 atoms, the device-wide sort above) so
+        that the first requests of each size do not wait for kernels to load."""
+        rng = np.random.default_rng(0)
+        for n in sizes:
+            side = int(np.ceil(n ** (1. / 3.)))
+            grid = np.stack(np.meshgrid(*[np.arange(side)] * 3, indexing='ij'), -1).reshape(-1, 3)[:n] * 2.5
+            structure = (grid + rng.normal(0., 0.05, grid.shape), np.full(n, 1.6))
+            handle = self.build([structure])[0]
+            self.trace([(handle, 12, 1)])
 
     def footprint(self, n_atoms):
         import ctypes as ct
