@@ -174,3 +174,44 @@ def test_batchccs_cap_ladder_stops_when_the_tail_is_small(eb):
             last = att[-1]
             assert last['tail_bound_angstrom2'] <= 5e-4 * last['ehss_angstrom2'] or last['cap'] == 64
             assert all(x['tail_bound_angstrom2'] > 5e-4 * x['ehss_angstrom2'] for x in att[:-1])
+
+
+def _shapes(seed):
+    """Structures of varied shape, density and radius mix for the exterior identity."""
+    rng = np.random.default_rng(seed)
+    out = []
+    # dense and sparse random clouds with mixed radii
+    for n, box in ((400, 12.), (400, 25.), (1500, 22.)):
+        c = rng.uniform(-box / 2, box / 2, (n, 3))
+        out.append((c, rng.uniform(0.6, 2.8, n)))
+    # a rod, a sheet, two separated clusters
+    t = rng.uniform(0, 60, 300)
+    out.append((np.stack([t, rng.normal(0, 1.2, 300), rng.normal(0, 1.2, 300)], 1), rng.uniform(1.2, 2.0, 300)))
+    out.append((np.stack([rng.uniform(0, 30, 500), rng.uniform(0, 30, 500), rng.normal(0, 0.8, 500)], 1),
+                np.full(500, 1.7)))
+    a = rng.normal(0, 3, (200, 3)); b = rng.normal(0, 3, (200, 3)) + [40., 0., 0.]
+    out.append((np.concatenate([a, b]), rng.uniform(1.0, 2.2, 400)))
+    # a dense ball of large atoms around a few small ones, with exact duplicates
+    c = rng.normal(0, 2.5, (250, 3))
+    c = np.concatenate([c, c[:20]])
+    out.append((c, np.concatenate([rng.uniform(1.5, 3.0, 250), rng.uniform(0.3, 0.6, 20)])))
+    return out
+
+
+@pytest.mark.parametrize('seed', [101, 202])
+def test_exterior_identity_on_varied_shapes(eb, seed):
+    """Exterior and full scenes give identical block results (FP32 filter, PA on)
+    on clouds, rods, sheets, split clusters and dense balls with duplicates."""
+    from ehss_b200.batch import BatchCCS
+    structures = _shapes(seed)
+    seeds = list(range(seed, seed + len(structures)))
+    kw = dict(repeats=2, cap=64, precision='fp32', pa=True, graph=False)
+    a = BatchCCS(structures, 14, seeds, exterior=False, **kw).run()
+    ext = BatchCCS(structures, 14, seeds, exterior=True, **kw)
+    b = ext.run()
+    keys = ('ehss_angstrom2', 'pa_angstrom2', 'unresolved_rays', 'escaped_rays', 'collision_histogram',
+            'collision_contribution_angstrom2')
+    for x, y in zip(a, b):
+        for rx, ry in zip(x['runs'], y['runs']):
+            assert {k: rx[k] for k in keys} == {k: ry[k] for k in keys}
+    assert sum(ext.batch.info(i).n_active for i in range(len(structures))) < sum(len(r) for _, r in structures)
