@@ -215,3 +215,23 @@ def test_exterior_identity_on_varied_shapes(eb, seed):
         for rx, ry in zip(x['runs'], y['runs']):
             assert {k: rx[k] for k in keys} == {k: ry[k] for k in keys}
     assert sum(ext.batch.info(i).n_active for i in range(len(structures))) < sum(len(r) for _, r in structures)
+
+
+@pytest.mark.parametrize('seed', [303])
+def test_fp32_filter_equals_fp64_on_varied_shapes(eb, seed):
+    """The FP32 filter with FP64 re-test returns the FP64 path's outcomes on the
+    varied shapes, also far from the origin and with radii spanning 0.1-3 A."""
+    from ehss_b200.batch import BatchCCS
+    rng = np.random.default_rng(seed)
+    structures = _shapes(seed)
+    c = rng.normal(0, 4, (300, 3)) + [1.0e4, -2.5e4, 3.0e3]          # far from the origin
+    structures.append((c, rng.uniform(0.1, 3.0, 300)))
+    seeds = list(range(seed, seed + len(structures)))
+    kw = dict(repeats=2, cap=64, pa=True, graph=False, exterior=False)
+    a = BatchCCS(structures, 14, seeds, precision='fp64', **kw).run()
+    b = BatchCCS(structures, 14, seeds, precision='fp32', **kw).run()
+    keys = ('ehss_angstrom2', 'pa_angstrom2', 'unresolved_rays', 'escaped_rays', 'collision_histogram',
+            'collision_contribution_angstrom2')
+    for x, y in zip(a, b):
+        for rx, ry in zip(x['runs'], y['runs']):
+            assert {k: rx[k] for k in keys} == {k: ry[k] for k in keys}
