@@ -177,3 +177,22 @@ def test_refit_refusals(eb):
     info = _lib.SceneInfo()
     assert lib.ehss_scene_info_get(ext.ptr, ct.byref(info), None) == _lib.ERR_VALUE
     assert b'refit requires a full' in lib.ehss_last_error()
+
+
+def test_refit_after_rigid_rotation_on_varied_shapes(eb):
+    """A rotated and translated copy refit into the old topology traces like a
+    rebuilt scene (per-ray outcomes) on clouds, rods, sheets and split clusters."""
+    from ehss_b200.state import Spheres
+    from test_gpu_batched import _shapes
+    rot = np.array([[0., -1., 0.], [1., 0., 0.], [0., 0., 1.]])
+    for i, (c0, r) in enumerate(_shapes(606)[:6]):
+        c1 = c0 @ rot.T + [7.5, -3.0, 120.0]
+        s = eb.Scene(c0, r)
+        s.refit(c1)
+        fresh = eb.Scene(c1, r)
+        _check_boxes(s)
+        src = eb.external_source(Spheres(c1, r, False), 11, 60 + i, scene=fresh)
+        got = eb.GPUEHSSTransport(s).trace(src, 64, record_history=True)
+        ref = eb.GPUEHSSTransport(fresh).trace(src, 64, record_history=True)
+        for name in ('positions', 'outgoing', 'escaped', 'unresolved', 'bounces', 'collider_ids'):
+            assert np.array_equal(getattr(got, name), getattr(ref, name)), (i, name)
