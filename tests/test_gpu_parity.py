@@ -477,3 +477,19 @@ def test_trace_matches_oracle_on_varied_shapes(eb):
         ref = O.StaticTree(c, r, 4).trace(src.origins, src.directions, cap=64, record=True, threads=O.host_cores())
         for field in ('positions', 'outgoing', 'escaped', 'unresolved', 'bounces', 'collider_ids'):
             np.testing.assert_array_equal(getattr(got, field), ref[field], err_msg=f'{i} {field}')
+
+
+def test_adaptive_pa_union_counts_on_varied_shapes(eb):
+    """The device's exact pixel unions equal the oracle's on the device's own
+    projected coordinates for clouds, rods, sheets, split clusters and dense
+    balls with duplicates."""
+    from ehss_b200.adaptive_pa import grid_counts
+    from test_gpu_batched import _shapes
+    for i, (c, r) in enumerate(_shapes(707)):
+        scene = eb.Scene(c, r)
+        ndir, grid = 8, 256
+        counts, spacing, xy = grid_counts(scene, ndir, grid, 11 + i, with_xy=True)
+        for k in range(ndir):
+            lower = np.array([-spacing[k] * grid / 2] * 2)
+            assert counts[k] == O.union_count(xy[k], r, lower, spacing[k], grid), (i, k)
+        assert np.all(counts > 0) and np.all(counts <= grid * grid)
