@@ -235,3 +235,23 @@ def test_fp32_filter_equals_fp64_on_varied_shapes(eb, seed):
     for x, y in zip(a, b):
         for rx, ry in zip(x['runs'], y['runs']):
             assert {k: rx[k] for k in keys} == {k: ry[k] for k in keys}
+
+
+def test_cap_extension_on_varied_shapes(eb):
+    """Cap 2 continued to 5, 17 and 64 equals a run at cap 64 on clouds, rods,
+    sheets, split clusters and dense balls with duplicates."""
+    from ehss_b200.blocks import BlockJob, BlockPlan
+    scenes = [eb.Scene(c, r, exterior=True) for c, r in _shapes(808)]
+    jobs = lambda cap: [BlockJob(sc, 12, 300 + s, cap=cap, pa=True, tag=(s, 0)) for s, sc in enumerate(scenes)]
+    plan = BlockPlan(jobs(2), residual_capacity=1 << 14)
+    plan.run()
+    first = plan.collect()
+    assert sum(r['unresolved_rays'] for r in first) > 10
+    ext = plan.extend_caps((5, 17, 64), tail_fraction=0.0)
+    ref = BlockPlan(jobs(64))
+    ref.run()
+    for a, b in zip(ext, ref.collect()):
+        for key in ('ehss_angstrom2', 'tail_bound_angstrom2', 'unresolved_rays', 'escaped_rays',
+                    'pa_from_same_rays_angstrom2', 'pa_angstrom2'):
+            assert a[key] == b[key], key
+        assert _padded(a, 64) == _padded(b, 64)
