@@ -3,6 +3,8 @@ with single-structure runs, the autotuner, and the served request loop."""
 import numpy as np
 import pytest
 
+from oracle import oracle as O
+
 pytestmark = pytest.mark.gpu
 
 
@@ -255,3 +257,26 @@ def test_cap_extension_on_varied_shapes(eb):
                     'pa_from_same_rays_angstrom2', 'pa_angstrom2'):
             assert a[key] == b[key], key
         assert _padded(a, 64) == _padded(b, 64)
+
+
+def test_large_structure_exterior_identity_and_oracle_ccs(eb):
+    """A 100,000-atom globule (device-wide key sort, global refit, exposure test
+    at scale): exterior and full scenes give identical blocks, and the CCS
+    equals the oracle's on the same rays."""
+    from ehss_b200 import workloads as W
+    from ehss_b200.batch import BatchCCS
+    c, r, _ = W.globule(100000, 1)
+    kw = dict(repeats=1, cap=64, pa=True, graph=False)
+    a = BatchCCS([(c, r)], 12, [9], exterior=False, **kw).run()[0]['runs'][0]
+    ext = BatchCCS([(c, r)], 12, [9], exterior=True, **kw)
+    b = ext.run()[0]['runs'][0]
+    for key in ('ehss_angstrom2', 'pa_angstrom2', 'unresolved_rays', 'escaped_rays', 'collision_histogram'):
+        assert a[key] == b[key], key
+    info = ext.batch.info(0)
+    assert info.n_active < info.n_atoms // 2                       # most of a large globule is buried
+    scene = eb.Scene(c, r)
+    o, d = (x.cpu().numpy() for x in scene.source_rays(12, 9))
+    ref = O.StaticTree(c, r, 4).trace(o, d, cap=64, threads=O.host_cores())
+    ro = O.readout(dict(incoming=d, weights=np.full(len(o), np.pi * scene.radius ** 2 / len(o))), ref, 64)
+    assert b['ehss_angstrom2'] == pytest.approx(ro['ehss_angstrom2'], rel=1e-12)
+    assert b['collision_histogram'] == ro['collision_histogram']
