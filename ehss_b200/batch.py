@@ -105,16 +105,32 @@ class BatchScenes:
         self.h2d_bytes = (N * 3 + N) * 8
 
     def upload(self):
+        self._require_build_buffers()
         self.d_xyz.copy_(self.h_xyz, non_blocking=True)
         self.d_r.copy_(self.h_r, non_blocking=True)
 
     def build(self, upload=True):
+        self._require_build_buffers()
         if upload:
             self.upload()
         lib = _lib.load()
         _lib.check(lib.ehss_scenes_build_ex(len(self.scenes), self._xyz_ptrs, self._r_ptrs, self._n, self.leaf_size,
                                             self._scenes, self._sizes, self.ws_ptr, self.ws_bytes, self.flags,
                                             stream_handle(self.device)), 'batched scene build')
+
+    def drop_build_buffers(self):
+        """Free the builder's workspace and the device coordinates once the
+        scenes are built (the served form keeps only the scene buffer).  The
+        memory returns to torch's stream-ordered cache, so the build queued
+        on this stream still finishes before anything reuses it.  Refit and
+        rebuild are unavailable afterwards."""
+        self.ws = self.d_xyz = self.d_r = self.h_xyz = self.h_r = None
+        self.ws_ptr = 0
+        self._xyz_ptrs = self._r_ptrs = None
+
+    def _require_build_buffers(self):
+        if self.ws is None:
+            raise RuntimeError('the build buffers of this batch were freed (drop_build_buffers)')
 
     def stage(self, structures):
         """Write new coordinates (and radii) of the same structures into the

@@ -22,7 +22,10 @@
 //     them on one stream;
 //   * the first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture begins.
+//     before any stream capture begins.  The address is kept per device and
+//     per CUDA context: after the context is torn down (cudaDeviceReset) the
+//     next call notices the new context and looks the address up again, so
+//     that call, too, belongs before any capture.
 #include <mutex>
 #include "ehss_internal.cuh"
 
@@ -39,9 +42,47 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+unsigned long long g_noalloc_ctx[kMaxDevices] = {0};
 
-// Device address of the scratch array for the current device (looked up
-// once per device, with that device current).
+// The address belongs to the device's context at the time of the lookup.  A
+// context that is torn down (cudaDeviceReset, or a driver-API caller
+// destroying it) takes the mapping with it, and the next context may map the
+// array elsewhere.  Each call therefore compares the current context's id
+// (cuCtxGetId: unique within the process, never reused) with the id recorded
+// at the lookup and looks the address up again when they differ.  Both driver
+// functions come through the runtime's entry-point query, so the library
+// does not link the driver library itself; without them every call looks the
+// address up.
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+
+bool current_context_id(unsigned long long* id) {
+    static bool tried = false;
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!tried) {
+        tried = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        const bool ok1 = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void**)&get_current, 12000,
+                                                          cudaEnableDefault, &q1) == cudaSuccess &&
+                         q1 == cudaDriverEntryPointSuccess;
+        const bool ok2 = cudaGetDriverEntryPointByVersion("cuCtxGetId", (void**)&get_id, 12000, cudaEnableDefault,
+                                                          &q2) == cudaSuccess &&
+                         q2 == cudaDriverEntryPointSuccess;
+        if (!ok1 || !ok2) {
+            get_current = nullptr;
+            get_id = nullptr;
+            cudaGetLastError();   // a failed query is not the caller's error
+        }
+    }
+    void* ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx) return false;
+    return get_id(ctx, id) == 0 && *id != 0;
+}
+
+// Device address of the scratch array for the current device: looked up
+// with that device current, at the device's first call and again after its
+// context has changed.
 int noalloc_scratch(void** out) {
     int dev = 0;
     int rc = cuda_status(cudaGetDevice(&dev), "current device");
@@ -51,11 +92,15 @@ int noalloc_scratch(void** out) {
         return EHSS_ERR_VALUE;
     }
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
+    unsigned long long id = 0;
+    const bool known = current_context_id(&id);
+    if (!known || !g_noalloc_ptr[dev] || g_noalloc_ctx[dev] != id) {
         void* p = nullptr;
         rc = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_scratch), "scratch symbol address");
         if (rc) return rc;
         g_noalloc_ptr[dev] = p;
+        // the lookup creates the primary context when none was current yet
+        g_noalloc_ctx[dev] = current_context_id(&id) ? id : 0;
     }
     *out = g_noalloc_ptr[dev];
     return EHSS_OK;

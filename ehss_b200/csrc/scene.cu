@@ -19,7 +19,8 @@
 //   3. stable sort of (key, atom) pairs, so equal codes keep atom order:
 //                  per structure in one CTA (k_morton_segsort, steps 2-3 in one
 //                  launch) when every structure holds at most 8192 atoms, else
-//                  CUB's device-wide radix sort
+//                  a device-wide LSD radix sort over the key's significant bits
+//                  (k_radix_count / k_radix_scan / k_radix_scatter, 8 bits a pass)
 //   4. k_karras    per internal node: Karras (2012) range / split search
 //                  within the structure's segment of tree atoms
 //   5. k_refit     per atom: FP32 boxes rounded outward, unioned bottom-up
@@ -33,7 +34,7 @@
 // repeat steps 2-6 with the buried atoms sorted behind the exposed ones and
 // left out of the tree.
 #include <cub/block/block_radix_sort.cuh>
-#include <cub/device/device_radix_sort.cuh>
+#include <cub/block/block_scan.cuh>
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -82,8 +83,8 @@ struct BuildWork {
     int32_t* inner_height;   // [I]
     uint32_t* arrivals;      // [I]
     uint8_t* culled;         // [N] 1 = buried atom (exterior builds)
-    void* cub_temp;
-    size_t cub_bytes;
+    uint32_t* radix_counts;  // [256 * tiles] per-tile digit counts of the device-wide sort
+    uint32_t* radix_offsets; // [256 * tiles] their exclusive scan (digit-major)
 };
 
 // --------------------------------------------------------------------------
@@ -273,6 +274,126 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_morton_segsort(cons
             vals_out[D.atom0 + j] = val[k];
         }
     }
+}
+
+// --------------------------------------------------------------------------
+// Device-wide stable LSD radix sort of (uint64 key, int32 value) pairs, for
+// batches with a structure above kSegSortMax atoms.  Each pass sorts by one
+// 8-bit digit in three launches:
+//   k_radix_count    per tile of kRadixTile keys: digit histogram, stored
+//                    digit-major (counts[digit * tiles + tile]);
+//   k_radix_scan     one CTA: exclusive scan of the counts in that order, so
+//                    offsets[digit * tiles + tile] is where the tile's keys
+//                    of that digit start in the output;
+//   k_radix_scatter  per tile: the tile's pairs are sorted by the digit in
+//                    shared memory (stable block radix sort of the blocked
+//                    arrangement, which is input order), and each pair goes
+//                    to its digit's offset plus its rank among the tile's
+//                    pairs of that digit.
+// Every pass is stable, so the result is the stable sort by the key's low
+// end_bit bits, element for element what any stable sort gives.
+// --------------------------------------------------------------------------
+constexpr int kRadixThreads = 256, kRadixItems = 8, kRadixTile = kRadixThreads * kRadixItems, kRadixBins = 256;
+static_assert(kRadixThreads == kRadixBins, "one thread per digit in the histogram steps");
+
+__host__ __device__ inline int64_t radix_tiles(int64_t n) { return (n + kRadixTile - 1) / kRadixTile; }
+
+__global__ void __launch_bounds__(kRadixThreads) k_radix_count(const uint64_t* keys, int64_t n, int shift,
+                                                              uint32_t* counts, int64_t tiles) {
+    __shared__ uint32_t h[kRadixBins];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kRadixTile;
+#pragma unroll
+    for (int k = 0; k < kRadixItems; ++k) {
+        const int64_t i = base + k * kRadixThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(unsigned)(keys[i] >> shift) & (kRadixBins - 1)], 1u);
+    }
+    __syncthreads();
+    counts[(int64_t)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(1024) k_radix_scan(const uint32_t* counts, uint32_t* offsets, int64_t m) {
+    // the counts add up to the batch's atom count (< 2^31), so 32-bit sums suffice
+    using Scan = cub::BlockScan<uint32_t, 1024>;
+    __shared__ typename Scan::TempStorage tmp;
+    const int64_t per = (m + 1023) / 1024;
+    const int64_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
+    uint32_t sum = 0;
+    for (int64_t i = b; i < e; ++i) sum += counts[i];
+    uint32_t pre;
+    Scan(tmp).ExclusiveSum(sum, pre);
+    for (int64_t i = b; i < e; ++i) {
+        const uint32_t c = counts[i];
+        offsets[i] = pre;
+        pre += c;
+    }
+}
+
+__global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const uint64_t* keys_in, const int32_t* vals_in,
+                                                                uint64_t* keys_out, int32_t* vals_out, int64_t n,
+                                                                int shift, const uint32_t* counts,
+                                                                const uint32_t* offsets, int64_t tiles) {
+    using Sort = cub::BlockRadixSort<uint64_t, kRadixThreads, kRadixItems, int32_t>;
+    using Scan = cub::BlockScan<uint32_t, kRadixThreads>;
+    __shared__ union {
+        typename Sort::TempStorage sort;
+        typename Scan::TempStorage scan;
+    } tmp;
+    __shared__ uint32_t start[kRadixBins], dest[kRadixBins];
+    const int64_t base = (int64_t)blockIdx.x * kRadixTile;
+    uint64_t key[kRadixItems];
+    int32_t val[kRadixItems];
+#pragma unroll
+    for (int k = 0; k < kRadixItems; ++k) {
+        const int64_t i = base + threadIdx.x * kRadixItems + k;     // blocked: item order = input order
+        const bool in = i < n;
+        key[k] = in ? keys_in[i] : ~0ull;                           // padding sorts behind every real key
+        val[k] = in ? vals_in[i] : -1;
+    }
+    // where this tile's keys of each digit start, in the tile and in the output
+    const int64_t slot = (int64_t)threadIdx.x * tiles + blockIdx.x;
+    uint32_t first;
+    Scan(tmp.scan).ExclusiveSum(counts[slot], first);
+    start[threadIdx.x] = first;
+    dest[threadIdx.x] = offsets[slot];
+    __syncthreads();
+    Sort(tmp.sort).Sort(key, val, shift, shift + 8 < 64 ? shift + 8 : 64);
+#pragma unroll
+    for (int k = 0; k < kRadixItems; ++k) {
+        if (val[k] < 0) continue;                                   // padding (last tile only)
+        const unsigned d = (unsigned)(key[k] >> shift) & (kRadixBins - 1);
+        const uint32_t pos = threadIdx.x * kRadixItems + k;           // rank in the sorted tile
+        const int64_t o = (int64_t)dest[d] + (pos - start[d]);
+        keys_out[o] = key[k];
+        vals_out[o] = val[k];
+    }
+}
+
+// Passes of the device-wide sort over bits [0, end_bit).
+__host__ __device__ inline int radix_passes(int end_bit) { return (end_bit + 7) / 8; }
+
+// Sorts n pairs; the input must be in (keys_a, vals_a) when the pass count is
+// odd and in (keys_b, vals_b) when it is even, so that the result always
+// lands in (keys_b, vals_b).
+static int radix_sort_pairs(uint64_t* keys_a, int32_t* vals_a, uint64_t* keys_b, int32_t* vals_b, int64_t n,
+                            int end_bit, uint32_t* counts, uint32_t* offsets, cudaStream_t stream) {
+    const int64_t tiles = radix_tiles(n);
+    const int passes = radix_passes(end_bit);
+    uint64_t* kin = passes % 2 ? keys_a : keys_b;
+    int32_t* vin = passes % 2 ? vals_a : vals_b;
+    uint64_t* kout = passes % 2 ? keys_b : keys_a;
+    int32_t* vout = passes % 2 ? vals_b : vals_a;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        k_radix_count<<<(unsigned)tiles, kRadixThreads, 0, stream>>>(kin, n, shift, counts, tiles);
+        k_radix_scan<<<1, 1024, 0, stream>>>(counts, offsets, (int64_t)kRadixBins * tiles);
+        k_radix_scatter<<<(unsigned)tiles, kRadixThreads, 0, stream>>>(kin, vin, kout, vout, n, shift, counts,
+                                                                        offsets, tiles);
+        uint64_t* tk = kin; kin = kout; kout = tk;
+        int32_t* tv = vin; vin = vout; vout = tv;
+    }
+    return cuda_status(cudaGetLastError(), "LBVH key sort");
 }
 
 // Karras (2012), "Maximizing parallelism in the construction of BVHs,
@@ -1101,13 +1222,6 @@ int upload_ico_tables(cudaStream_t stream) {
 }
 
 }  // namespace
-static size_t cub_sort_bytes(int64_t N) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint64_t*)nullptr, (uint64_t*)nullptr,
-                                    (const int32_t*)nullptr, (int32_t*)nullptr, (int)(N > 0 ? N : 1));
-    return bytes;
-}
-
 // Workspace for a batch with N atoms over S structures.
 uint64_t build_workspace_bytes(int64_t N, int S) {
     int64_t I = N > 0 ? N : 1;
@@ -1125,7 +1239,7 @@ uint64_t build_workspace_bytes(int64_t N, int S) {
     b += align256(4ull * I);            // inner_height
     b += align256(4ull * I);            // arrivals
     b += align256(1ull * N);            // culled
-    b += align256(cub_sort_bytes(N));
+    b += 2 * align256(4ull * kRadixBins * (uint64_t)radix_tiles(N));   // radix counts, offsets
     return b + 256;
 }
 
@@ -1194,8 +1308,8 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
     W.inner_height = (int32_t*)p; p += align256(4ull * Ia);
     W.arrivals = (uint32_t*)p; p += align256(4ull * Ia);
     W.culled = (uint8_t*)p; p += align256(1ull * N);
-    W.cub_temp = p;
-    W.cub_bytes = cub_sort_bytes(N);
+    W.radix_counts = (uint32_t*)p; p += align256(4ull * kRadixBins * (uint64_t)radix_tiles(N));
+    W.radix_offsets = (uint32_t*)p;
 
     // The headers are written on the device (k_stats); the descriptors are the
     // only upload.  A copy from pageable host memory has staged its source
@@ -1222,10 +1336,12 @@ int build_scenes(int S, const double* const* xyz, const double* const* radii, co
                 k_morton_segsort<512, 16><<<S, 512, 0, stream>>>(W.descs, culled, W.keys_out, W.vals_out);
             r = cuda_status(cudaGetLastError(), "LBVH key sort");
         } else {
-            k_morton<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, culled, W.keys_in, W.vals_in);
-            size_t cub_bytes = W.cub_bytes;
-            r = cuda_status(cub::DeviceRadixSort::SortPairs(W.cub_temp, cub_bytes, W.keys_in, W.keys_out, W.vals_in,
-                                                            W.vals_out, (int)N, 0, end_bit, stream), "LBVH key sort");
+            // the keys start in the buffer from which an odd or even number of passes ends in keys_out
+            const bool odd = radix_passes(end_bit) % 2 != 0;
+            k_morton<<<blocks(N), T, 0, stream>>>(W.descs, W.atom_scene, N, culled, odd ? W.keys_in : W.keys_out,
+                                                  odd ? W.vals_in : W.vals_out);
+            r = radix_sort_pairs(W.keys_in, W.vals_in, W.keys_out, W.vals_out, N, end_bit, W.radix_counts,
+                                 W.radix_offsets, stream);
         }
         if (r) return r;
         // parent links start at -1 so that a missing link ends a refit walk

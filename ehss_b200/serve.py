@@ -40,10 +40,20 @@ class CCSRequest:
 
 
 @dataclass
+class BuildGroup:
+    """Requests admitted together share one device allocation (one batched
+    build), which is freed only when the last of them finishes; the group's
+    bytes stay counted against the budget until then."""
+    bytes: int
+    members: int
+
+
+@dataclass
 class RequestState:
     req: CCSRequest
     footprint: int
     handle: object = None
+    group: BuildGroup = None
     values: list = field(default_factory=list)
     tails: list = field(default_factory=list)
     admitted_at: float = None
@@ -99,10 +109,21 @@ class CCSServer:
         self.pending = keep
         if admitted:
             handles = self.ex.build([(s.req.centers, s.req.radii) for s in admitted])
+            group = BuildGroup(sum(s.footprint for s in admitted), len(admitted))
             for s, h in zip(admitted, handles):
                 s.handle = h
+                s.group = group
             self.active.extend(admitted)
         return admitted
+
+    def _finish(self, s):
+        """A finished request drops its handle; its group's memory returns to
+        the budget when the group's last member has finished."""
+        self.ex.release(s.handle)
+        s.handle = None
+        s.group.members -= 1
+        if s.group.members == 0:
+            self.used -= s.group.bytes
 
     def step(self):
         """Admit what has arrived and fits, then run one round; returns requests completed."""
@@ -130,8 +151,7 @@ class CCSServer:
             if (len(s.values) >= self.min_blocks and rel_rmse(s.values) <= self.target) or \
                     len(s.values) >= self.max_blocks:
                 s.done_at = now
-                self.used -= s.footprint
-                self.ex.release(s.handle)
+                self._finish(s)
                 a = np.asarray(s.values)
                 self.done[s.req.rid] = dict(rid=s.req.rid, atoms=len(s.req.radii), ehss_mean_angstrom2=float(a.mean()),
                                             sd=float(a.std(ddof=1)) if len(a) > 1 else None, rel_rmse=rel_rmse(a),
@@ -196,17 +216,22 @@ class DeviceExecutor:
             self.trace([(handle, 12, 1)])
 
     def footprint(self, n_atoms):
+        """Device bytes one request may hold: its scene, its share of the
+        build workspace and its coordinates and radii (32 B per atom).  The
+        server counts them for every member of a batched build until the
+        batch's last request finishes, so the budget bounds what is allocated."""
         import ctypes as ct
         from . import _lib
         sb, wb = ct.c_uint64(), ct.c_uint64()
         _lib.check(_lib.load().ehss_scene_bytes(int(n_atoms), self.leaf_size, ct.byref(sb), ct.byref(wb)))
-        return int(sb.value + wb.value)
+        return int(sb.value + wb.value + 32 * int(n_atoms) + 512)
 
     def build(self, structures):
         from .batch import BatchScenes
         # every block ray starts on the impact disk: exterior scenes give the same outcomes
         scenes = BatchScenes(structures, leaf_size=self.leaf_size, device=self.device, exterior=True)
         scenes.build()
+        scenes.drop_build_buffers()
         return [(scenes, i) for i in range(len(structures))]
 
     def trace(self, jobs):
@@ -218,4 +243,4 @@ class DeviceExecutor:
         return [(r['ehss_angstrom2'], r['tail_bound_angstrom2']) for r in res]
 
     def release(self, handle):
-        pass    # the batch's buffers go when its last request is released (reference counting by Python)
+        pass    # the batch's scene buffer goes with the last handle into it (the server drops each handle)

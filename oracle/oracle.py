@@ -210,9 +210,15 @@ P = ct.c_void_p
 I64 = ct.c_int64
 
 
-def build():
-    """Compile liboracle.so (and the reference's own kernel where present)."""
-    subprocess.run(['make', '-s', '-C', str(HERE)], check=True)
+def build(reference=None):
+    """Compile liboracle.so and, when ``reference`` (or the EHSS_REFERENCE
+    environment variable) names a reference checkout, the reference's own
+    C++ kernel into _ref/."""
+    cmd = ['make', '-s', '-C', str(HERE)]
+    reference = reference or os.environ.get('EHSS_REFERENCE')
+    if reference:
+        cmd.append(f'REF={reference}')
+    subprocess.run(cmd, check=True)
 
 
 def lib():

@@ -2,7 +2,7 @@
 
 Run once, in a container that holds the SCIMMS/EHSS reference tree:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout>
 
 It imports the reference's own Python package (its Numba kernels, scipy's
 Sobol generator and its CLI helpers) and records their outputs on small,
@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -67,10 +68,13 @@ def compact_fixtures(Spheres):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--reference', default=os.environ.get('EHSS_REFERENCE'),
+                    help='reference checkout (default: the EHSS_REFERENCE environment variable)')
     ap.add_argument('--only', choices=['compact'], default=None,
                     help='regenerate one fixture file only (the others stay as they are)')
     args = ap.parse_args()
+    if not args.reference:
+        ap.error('name the reference checkout with --reference or EHSS_REFERENCE')
     sys.path.insert(0, str(Path(args.reference) / 'src'))
     from scipy.stats import qmc
     from support_exchange_transport.inside_out_pa import Spheres, Source

@@ -438,26 +438,75 @@ def test_config_globule650_fp64_per_ray_20_seeds(eb):
         np.testing.assert_array_equal(blocked, patree.query(src.origins, src.directions, threads=O.host_cores())[0])
 
 
-def test_config_globule2000_fp32_precision(eb):
-    """2000-atom globule, 262,144 rays per seed through the fused FP32 kernel
-    with FP64 re-test: CCS within 1e-12 of the FP64 oracle on the same rays,
-    identical bounce histograms, grazing queries counted."""
+def _per_ray_fp32_config(eb, n_atoms, log2, seeds, structure_seed):
+    """One configuration in the FP32 filter with FP64 re-test, every seed
+    traced twice on the device: per ray through the explicit-ray kernel
+    (engine.trace, full scene) and as fused blocks (all seeds in one
+    persistent launch, exterior scene).  Both are compared with the oracle
+    on the device's own rays.  Returns the per-configuration totals."""
     from ehss_b200 import workloads as W
-    from ehss_b200.blocks import BlockJob, BlockPlan, DEFAULT_LAUNCH
-    c, r, _ = W.globule(2000, 2000)
-    scene = eb.Scene(c, r, exterior=True)
+    from ehss_b200.blocks import BlockJob, BlockPlan
+    c, r, _ = W.globule(n_atoms, structure_seed)
+    s = eb.Spheres(c, r, deduplicate=False)
+    prep = eb.PreparedStaticGPUEHSS(s, precision='fp32')
+    ext = eb.Scene(c, r, exterior=True)
+    plan = BlockPlan([BlockJob(ext, log2, seed, cap=64, tag=seed) for seed in seeds])
+    plan.run()
+    fused = {res['tag']: res for res in plan.collect()}
     tree = O.StaticTree(c, r, 4)
-    for seed in (0, 1):
-        plan = BlockPlan([BlockJob(scene, 18, seed, cap=64)], launch=dict(DEFAULT_LAUNCH, count_tests=True))
-        plan.run()
-        got = plan.collect()[0]
-        o, d = (x.cpu().numpy() for x in scene.source_rays(18, seed))
-        ref = tree.trace(o, d, cap=64, threads=O.host_cores())
-        ro = O.readout(dict(incoming=d, weights=np.full(len(o), np.pi * scene.radius ** 2 / len(o))), ref, 64)
-        assert abs(got['ehss_angstrom2'] - ro['ehss_angstrom2']) <= 1e-12 * ro['ehss_angstrom2']
-        assert got['collision_histogram'] == ro['collision_histogram']
-        assert got['unresolved_rays'] == ro['unresolved_rays']
-        assert got['grazing_queries'] >= 0 and got['queries'] > len(o)
+    cores = O.host_cores()
+    tot = dict(rays=0, queries=0, grazing=0, fallback=0, disagreements=0, hit_rays=0, worst_rel_err=0.0)
+    hist = np.zeros(65, dtype=np.int64)
+    for seed in seeds:
+        src = eb.external_source(s, log2, seed, scene=prep.scene)
+        got = prep.engine.trace(src, 64)
+        ref = tree.trace(src.origins, src.directions, cap=64, threads=cores)
+        bad = ((got.escaped != ref['escaped']) | (got.unresolved != ref['unresolved'])
+               | (got.bounces != ref['bounces']) | np.any(got.outgoing != ref['outgoing'], axis=1)
+               | np.any(got.positions != ref['positions'], axis=1))
+        hit = (got.bounces > 0) | got.unresolved
+        np.testing.assert_array_equal(hit, (ref['bounces'] > 0) | ref['unresolved'], err_msg=f'seed {seed} hit flags')
+        m = got.metrics
+        tot['rays'] += len(hit)
+        tot['queries'] += m['queries']
+        tot['grazing'] += m['grazing_queries']
+        tot['fallback'] += m['fp64_fallback_queries']
+        tot['disagreements'] += int(bad.sum())
+        tot['hit_rays'] += int(hit.sum())
+        hist += np.bincount(ref['bounces'], minlength=65)[:65]
+        ro = O.readout(dict(incoming=src.incoming, weights=src.weights), ref, 64)
+        rel = abs(fused[seed]['ehss_angstrom2'] - ro['ehss_angstrom2']) / ro['ehss_angstrom2']
+        tot['worst_rel_err'] = max(tot['worst_rel_err'], rel)
+        assert rel <= 1e-12, (seed, rel)
+        assert fused[seed]['collision_histogram'] == ro['collision_histogram'], seed
+        assert fused[seed]['unresolved_rays'] == ro['unresolved_rays'], seed
+        assert got.tail_bound == pytest.approx(ro['tail_bound_angstrom2'], rel=1e-15, abs=0)
+    print(f"\n{n_atoms} atoms, {len(seeds)} x 2^{log2} rays (FP32 filter + FP64 re-test): "
+          f"{tot['disagreements']} per-ray disagreements (grazing rays included), "
+          f"{tot['grazing']} grazing and {tot['fallback']} fallback queries of {tot['queries']}, "
+          f"CCS rel err <= {tot['worst_rel_err']:.2e}, bounce histogram {hist[:12].tolist()}...")
+    return tot, hist
+
+
+def test_config_globule2000_fp32_per_ray_20_seeds(eb):
+    """2000-atom globule, 262,144 rays x 20 seeds: FP32 traversal and
+    intersection with FP64 near-tangent re-test.  Every ray's hit flag,
+    bounce count, final position and exit direction equal the FP64 oracle's
+    on the same rays (grazing disagreements counted: zero by construction,
+    since every sphere within the filter's error band is re-tested in FP64);
+    each seed's fused-block CCS is within 1e-12 of the oracle's."""
+    tot, hist = _per_ray_fp32_config(eb, 2000, 18, range(20), 2000)
+    assert tot['disagreements'] == 0
+    assert tot['rays'] == 20 << 18 and tot['queries'] > tot['rays']
+    # a hit ray bounced at least once (an unresolved ray stopped at the cap)
+    assert hist.sum() == tot['rays'] and hist[1:].sum() == tot['hit_rays']
+
+
+def test_config_globule650_fp32_per_ray_20_seeds(eb):
+    """650-atom globule, 65,536 rays x 20 seeds in the FP32 filter: per-ray
+    outcomes identical to the oracle's, fused CCS within 1e-12."""
+    tot, _ = _per_ray_fp32_config(eb, 650, 16, range(20), 650)
+    assert tot['disagreements'] == 0 and tot['rays'] == 20 << 16
 
 
 def test_trace_matches_oracle_on_varied_shapes(eb):

@@ -3,6 +3,8 @@ header declares, the host Sobol scrambler is bit-exact, block preparation,
 argument validation, workload generators and the reference data types."""
 import ctypes as ct
 
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -67,6 +69,18 @@ def test_argument_validation_without_device(lib):
                                     1 << 20, 1, None) == _lib.ERR_VALUE
     with pytest.raises(ValueError):
         _lib.check(_lib.ERR_VALUE)
+
+
+def test_noalloc_limit_fits_the_fixed_scratch_array(lib):
+    """The allocation-free build's stated maximum (EHSS_NOALLOC_MAX_ATOMS)
+    must fit its fixed 4 MiB workspace; the workspace size is host arithmetic
+    (the builder's own sort has no size that depends on a library version)."""
+    limit = 20000
+    sb, wb = ct.c_uint64(), ct.c_uint64()
+    assert lib.ehss_scene_bytes(limit, 16, ct.byref(sb), ct.byref(wb)) == 0
+    assert wb.value <= 4 << 20
+    header = (Path(__file__).resolve().parents[1] / 'include' / 'ehss_b200.h').read_text()
+    assert f'#define EHSS_NOALLOC_MAX_ATOMS {limit}' in header
 
 
 def test_blocks_prepare_chunks_and_offsets(lib):

@@ -85,6 +85,39 @@ def test_admission_by_memory_and_rejection():
         server.submit(_req('huge', 5000))
 
 
+def test_batch_memory_held_until_its_last_member_finishes():
+    """Two requests admitted together share one build allocation: when the
+    quick one finishes, its bytes stay counted until the slow one is done, so
+    a third request that fits only in the freed share waits for the batch."""
+    class TwoSpeed(FakeExecutor):
+        def trace(self, jobs):
+            # 'quick' (10 atoms) converges at once; 'slow' (20 atoms) needs 6 blocks
+            out = []
+            for (n, key), log2, seed in jobs:
+                if n == 10:
+                    out.append((100.0, 0.0))
+                else:
+                    out.append((100.0 + (20.0 if seed % 2 else -20.0), 0.0))
+            return out
+    ex = TwoSpeed()
+    server = CCSServer(ex, budget_bytes=100 * 35, target=0.1, max_blocks=6)
+    server.submit(_req('quick', 10))
+    server.submit(_req('slow', 20))
+    server.submit(_req('third', 10))        # fits only in what 'quick' held
+    server.step()
+    assert 'quick' in server.done and [s.req.rid for s in server.active] == ['slow']
+    assert server.used == 100 * 30          # the batch is still allocated
+    server.step()
+    assert [s.req.rid for s in server.pending] == ['third']
+    while 'slow' not in server.done:
+        server.step()
+    assert server.used == 0 or [s.req.rid for s in server.active] == ['third']
+    done = server.run()
+    assert set(done) == {'quick', 'slow', 'third'}
+    assert done['third']['admitted_s'] >= done['slow']['latency_s'] - 1e-9
+    assert server.used == 0
+
+
 def test_late_arrivals_join_running_rounds():
     t = [0.0]
     ex = FakeExecutor(noise=0.05)

@@ -32,8 +32,9 @@ def test_noalloc_build_matches_allocating_build():
     lib = _lib.load()
     stream = stream_handle()
     for call in range(2):
-        # 12,000 atoms take the device-wide key sort, whose temporary storage also comes from the array
-        for n, seed in ((650, 1 + call), (23, 7), (1, 3), (12000, 5)):
+        # above 8192 atoms the keys go through the device-wide sort, whose counters also live in the
+        # array; 20,000 atoms is the stated maximum
+        for n, seed in ((650, 1 + call), (23, 7), (1, 3), (12000, 5), (20000, 8 + call)):
             c, r, _ = W.globule(n, seed)
             xyz = torch.from_numpy(np.ascontiguousarray(c)).cuda()
             rad = torch.from_numpy(np.ascontiguousarray(r)).cuda()
