@@ -32,4 +32,14 @@ def test_bench_prints_the_contract_line():
     assert roof['achieved'] > 0 and roof['peak'] > 0 and 0 < roof['frac'] < 1.5 and roof['kernel_ms'] > 0
     assert d['gpu_launches'] == 15 * 3
     assert d['ccs_rel_err_max_vs_fp64_oracle'] <= 1e-5
+    # every timed block checked against the oracle on its own rays
+    ccs = d['ccs_vs_fp64_oracle']
+    assert ccs['blocks_checked'] == ccs['blocks'] == 16 * 3 and ccs['structure_rel_err_max'] <= 1e-5
+    assert roof['ref_sphere_tests_per_ray'] > 0 and roof['ref_box_tests_per_ray'] > 0
+    for name in ('C1_triatomic', 'C2_globule650', 'C3_globule2000'):
+        c = d['configs'][name]
+        assert c['rays_per_s'] > 0 and 0 < c['roofline_frac'] < 1.5 and c['ccs_rel_err_max_vs_fp64_oracle'] <= 1e-5
+        assert sum(c['bounce_histogram']) == c['rays']
+    assert d['configs']['C2_globule650']['pa_blocked_rays_equal_oracle'] is True
+    assert d['e2e_explicit']['rays_per_s'] > 0
     assert d['plain']['rays_per_s'] > 0 and d['batched_over_plain'] > 0
