@@ -826,6 +826,8 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                                 atomicAdd(&A.pa, 1u);
                                 if (RAYS) atomicAdd(&A.pa_fx, __double2ull_rn(*rho_lane * kFxScale));
                             }
+                            // the counting instance adds the any-hit tests to the block's counters
+                            if (COUNT) { W.box += pst.box; W.sphere += pst.sphere; }
                         }
                         bounces = 0;
                         last_rank = -1;

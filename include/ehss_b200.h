@@ -320,7 +320,8 @@ typedef struct ehss_launch {
                                  (0 = 16, max 32); deeper entries go to local memory */
     int32_t reserved;         /* 0 */
 } ehss_launch;
-#define EHSS_LAUNCH_COUNT_TESTS 1   /* count box and sphere tests into the block stats (slower) */
+#define EHSS_LAUNCH_COUNT_TESTS 1   /* count box and sphere tests into the block stats (slower); a block
+                                       with EHSS_BLOCK_PA adds its any-hit tests to the same counters */
 #define EHSS_LAUNCH_RAY_BLOCKS 2    /* some blocks have EHSS_BLOCK_RAYS (adds a launch of that kernel instance) */
 #define EHSS_LAUNCH_NO_DISK_BLOCKS 4  /* with EHSS_LAUNCH_RAY_BLOCKS: every block has EHSS_BLOCK_RAYS */
 

@@ -66,11 +66,169 @@ def compact_fixtures(Spheres):
     np.savez_compressed(HERE / 'compact.npz', **comp)
 
 
+# Error cases of the reference CLI: (kind, input, ...) -> the message it raises.
+BAD_ARGS = [
+    ['--rays', '1000'], ['--rays', '4'], ['--rays', str(2 ** 23)], ['--directions', '3'], ['--directions', '0'],
+    ['--grid-size', '4'], ['--grid-size', '16384'], ['--repeats', '0'], ['--threads', '0'], ['--leaf-size', '0'],
+    ['--max-collisions', '0'], ['--frame', '0'], ['--max-collisions', '100001'], ['--seed', '-1'],
+    ['--seed', str(2 ** 32)], ['--probe-radius', '-0.5'], ['--probe-radius', 'nan'], ['--probe-radius', 'inf'],
+    ['--rays', '1000', '--repeats', '0'], ['--repeats', '0', '--seed', '-1'],
+]
+BAD_XYZ = {
+    'empty': '\n\n',
+    'count': 'x\ncomment\nC 0 0 0\n',
+    'zero': '0\ncomment\n',
+    'short': '2\ncomment\nC 0 0 0\n',
+    'extended': '1\nLattice="1 0 0 0 1 0 0 0 1" Properties=species:S:1\nC 0 0 0\n',
+    'fields': '1\ncomment\nC 0 0\n',
+    'fields5': '1\ncomment\nC 0 0 0 7\n',
+    'symbol': '1\ncomment\nC1 0 0 0\n',
+    'number': '1\ncomment\nC 0 zero 0\n',
+    'finite': '1\ncomment\nC 0 inf 0\n',
+    'second_frame': '1\na\nC 0 0 0\n2\nb\nC 0 0 0\n',
+    'second_frame_row': '1\na\nC 0 0 0\n\n1\nb\nO 1 2\n',
+}
+GOOD_XYZ = {
+    'fortran_exponent': '2\nfortran\nc 1.0D0 0 0\nO 0 2.5d-1 0\n',
+    'frames_and_blanks': '\n1\na\nC 0 0 0\n\n\n2\nb b\nC 0 0 0\nN 1 0 0\n',
+    'bom': '\ufeff1\nbom\nS 0 0 0\n',
+}
+BAD_RADII = {'list': [1, 2], 'empty': {}, 'symbol': {'C12': 1.0}, 'duplicate': {'C': 1.7, 'c': 1.6},
+             'negative': {'C': -1.0}, 'bool': {'C': True}, 'string': {'C': '1.7'}, 'zero': {'N': 0}}
+
+
+def cli_interface_fixtures(ccs_cli):
+    """The reference CLI's messages and output layout (cli_interface.json):
+    argument validation, XYZ parsing, radii JSON and frame preparation
+    errors, parsed frames of accepted inputs, the default settings, and the
+    key sets and CSV header of a full run's output files."""
+    import tempfile
+    out = dict(args={}, xyz={}, xyz_ok={}, radii={}, frames={},
+               inputs=dict(xyz=BAD_XYZ, xyz_ok=GOOD_XYZ, radii=BAD_RADII))
+    for argv in BAD_ARGS:
+        a = ccs_cli.parser().parse_args(['x.xyz', '--output', '/nonexistent/out', *argv])
+        try:
+            ccs_cli.validate_args(a)
+            out['args'][' '.join(argv)] = None
+        except ValueError as exc:
+            out['args'][' '.join(argv)] = str(exc)
+    with tempfile.TemporaryDirectory() as tmp:
+        tmp = Path(tmp)
+        a = ccs_cli.parser().parse_args(['x.xyz', '--output', str(tmp)])
+        try:
+            ccs_cli.validate_args(a)
+        except ValueError as exc:
+            out['args']['<existing output>'] = str(exc).replace(str(tmp), '{output}')
+        for name, text in BAD_XYZ.items():
+            f = tmp / f'{name}.xyz'
+            f.write_text(text, encoding='utf-8')
+            try:
+                ccs_cli.read_xyz(f)
+                out['xyz'][name] = None
+            except ValueError as exc:
+                out['xyz'][name] = str(exc).replace(str(f), '{path}')
+        for name, text in GOOD_XYZ.items():
+            f = tmp / f'{name}.xyz'
+            f.write_text(text, encoding='utf-8')
+            out['xyz_ok'][name] = [dict(number=fr.number, comment=fr.comment, elements=list(fr.elements),
+                                        coordinates=fr.coordinates.tolist()) for fr in ccs_cli.read_xyz(f)]
+        for name, raw in BAD_RADII.items():
+            f = tmp / f'{name}.json'
+            f.write_text(json.dumps(raw), encoding='utf-8')
+            try:
+                ccs_cli.radius_table(f)
+                out['radii'][name] = None
+            except ValueError as exc:
+                out['radii'][name] = str(exc)
+        table = ccs_cli.radius_table(None)
+        frame = ccs_cli.XYZFrame
+        cases = {
+            'only_h_excluded': (frame(1, 'h', ('H', 'H'), np.array([[0., 0, 0], [1, 0, 0]])), dict(exclude_hydrogen=True)),
+            'unknown': (frame(2, 'u', ('C', 'Xe', 'Au'), np.array([[0., 0, 0], [1, 0, 0], [2, 0, 0]])), {}),
+            'coincident': (frame(3, 'c', ('C', 'O'), np.array([[1., 2, 3], [1, 2, 3]])), {}),
+            'overflow': (frame(1, 'o', ('C', 'O'), np.array([[0., 0, 0], [1e308, 0, 0]])), dict(units='nm')),
+            'ok_nm': (frame(4, 'ok', ('O', 'H', 'H'), np.array([[0.1, 0, 0], [0.2, 0.05, 0], [0, 0.3, 0.01]])),
+                      dict(units='nm')),
+            'ok_noh': (frame(5, 'ok', ('O', 'H', 'C'), np.array([[3., 1, 0], [2, 0.5, 0], [0, 3, 0.1]])),
+                       dict(exclude_hydrogen=True)),
+        }
+        for name, (fr, kw) in cases.items():
+            try:
+                spheres, info = ccs_cli.prepare_frame(fr, table, 1.4, **kw)
+                out['frames'][name] = dict(centers=spheres.centers.tolist(), radii=spheres.radii.tolist(), info=info)
+            except ValueError as exc:
+                out['frames'][name] = str(exc)
+        # a full run on a one-atom file: the output files' layout
+        xyz = tmp / 'single_carbon.xyz'
+        xyz.write_text('1\nsingle carbon\nC 0 0 0\n', encoding='utf-8')
+        run = tmp / 'run'
+        assert ccs_cli.main([str(xyz), '--rays', '1024', '--directions', '8', '--grid-size', '64', '--repeats', '2',
+                             '--output', str(run)]) == 0
+        payload = json.loads((run / 'results.json').read_text(encoding='utf-8'))
+        rec = payload['records'][0]
+        out['results'] = dict(top=sorted(payload), record=sorted(rec), summary=sorted(rec['summary']),
+                              run=sorted(rec['runs'][0]), run_pa=sorted(rec['runs'][0]['pa']),
+                              run_ehss=sorted(rec['runs'][0]['ehss']), timings=sorted(rec['timings']),
+                              settings=payload['settings'], notes=payload['notes'],
+                              radii_source=payload['radii_source'], radii=payload['atomic_radii_angstrom'])
+        bvh = tmp / 'bvh'
+        assert ccs_cli.main([str(xyz), '--rays', '1024', '--repeats', '1', '--pa-method', 'bvh',
+                             '--output', str(bvh)]) == 0
+        rec = json.loads((bvh / 'results.json').read_text(encoding='utf-8'))['records'][0]
+        out['results']['run_pa_bvh'] = sorted(rec['runs'][0]['pa'])
+        out['results']['run_bvh'] = sorted(rec['runs'][0])
+        header = (run / 'summary.csv').read_text(encoding='utf-8-sig').splitlines()[0]
+        out['results']['csv_header'] = header.split(',')
+    out['default_settings'] = {k: (str(v) if isinstance(v, Path) else v)
+                               for k, v in vars(ccs_cli.parser().parse_args(['x.xyz'])).items()}
+    (HERE / 'cli_interface.json').write_text(json.dumps(out, indent=1, ensure_ascii=False) + '\n', encoding='utf-8')
+
+
+# Reference structures (PDB-derived heavy-atom XYZ files shipped with the
+# reference) traced by the reference CLI's solve_frame.
+STRUCTURES = [('1AL1', [64]), ('1CLL', [64]), ('1AO6', [64]), ('1BMF', [64, 512])]
+
+
+def structure_fixtures(ccs_cli, reference):
+    """structures.npz: each structure's XYZ text; structures.json: the
+    prepared spheres' digest and the reference's solve_frame readouts
+    (EHSS + BVH PA, 16,384 rays x 3 replicates, seed 190003) at each cap."""
+    import hashlib
+    texts, readouts = {}, {}
+    table = ccs_cli.radius_table(None)
+
+    def strip(obj):
+        if isinstance(obj, dict):
+            return {k: strip(v) for k, v in obj.items() if not k.endswith('_s')}
+        if isinstance(obj, list):
+            return [strip(v) for v in obj]
+        return obj
+    for name, caps in STRUCTURES:
+        path = reference / 'data' / 'inputs' / 'evaluation18' / f'{name}.xyz'
+        raw = path.read_bytes()
+        texts[name] = np.frombuffer(raw, dtype=np.uint8)
+        frame = ccs_cli.read_xyz(path)[0]
+        spheres, info = ccs_cli.prepare_frame(frame, table, 1.4)
+        entry = dict(atoms=len(spheres.radii), comment=info['comment'],
+                     centers_sha256=hashlib.sha256(np.ascontiguousarray(spheres.centers).tobytes()).hexdigest(),
+                     radii_sha256=hashlib.sha256(np.ascontiguousarray(spheres.radii).tobytes()).hexdigest(),
+                     runs={})
+        for cap in caps:
+            argv = ['unused.xyz', '--method', 'both', '--pa-method', 'bvh', '--rays', '16384', '--repeats', '3',
+                    '--max-collisions', str(cap), '--output', '/nonexistent/x']
+            out = ccs_cli.solve_frame(spheres, ccs_cli.parser().parse_args(argv), False)
+            entry['runs'][str(cap)] = dict(argv=argv, summary=out['summary'], runs=strip(out['runs']))
+        readouts[name] = entry
+        print(name, len(spheres.radii), 'atoms', {c: r['summary']['ehss_angstrom2']['mean'] for c, r in entry['runs'].items()})
+    np.savez_compressed(HERE / 'structures.npz', **texts)
+    (HERE / 'structures.json').write_text(json.dumps(readouts, indent=1) + '\n')
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--reference', default=os.environ.get('EHSS_REFERENCE'),
                     help='reference checkout (default: the EHSS_REFERENCE environment variable)')
-    ap.add_argument('--only', choices=['compact'], default=None,
+    ap.add_argument('--only', choices=['compact', 'cli'], default=None,
                     help='regenerate one fixture file only (the others stay as they are)')
     args = ap.parse_args()
     if not args.reference:
@@ -86,6 +244,11 @@ def main():
     if args.only == 'compact':
         compact_fixtures(Spheres)
         print('wrote compact.npz')
+        return
+    if args.only == 'cli':
+        cli_interface_fixtures(ccs_cli)
+        structure_fixtures(ccs_cli, Path(args.reference))
+        print('wrote cli_interface.json, structures.json, structures.npz')
         return
 
     # ---- Sobol -------------------------------------------------------------
@@ -242,6 +405,8 @@ def main():
         cli[name] = dict(argv=argv, centers=s.centers.tolist(), radii=s.radii.tolist(),
                          summary=out['summary'], runs=strip(out['runs']))
     (HERE / 'cli.json').write_text(json.dumps(cli, indent=1) + '\n')
+    cli_interface_fixtures(ccs_cli)
+    structure_fixtures(ccs_cli, Path(args.reference))
     compact_fixtures(Spheres)
     print('wrote', sorted(p.name for p in HERE.glob('*.npz')), 'cli.json')
 
