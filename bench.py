@@ -90,7 +90,10 @@ def config(args, world):
             "structures_per_gpu": args.structures, "replicates": REPEATS, "cap": CAP,
             "precision": "fp32 traversal + fp64 re-test", "master_seed": MASTER_SEED,
             "scenes": "exterior (buried atoms left out of the trees; outcomes unchanged)",
-            "l2": "flushed (256 MB write) between timed steps", "host": "gc.freeze() after set-up", "parallelism": f"replicas x{world} (weak)"}
+            "l2": "flushed (256 MB write) between timed steps", "host": "gc.freeze() after set-up",
+            "parallelism": "1 GPU" if world == 1 else
+            f"one job of {args.structures * world} structures over {world} GPUs: LPT structure shards, "
+            "NCCL all-reduce of the block integers in every step (weak: structures per GPU fixed)"}
 
 
 # ----------------------------------------------------------------------------
@@ -480,7 +483,20 @@ def main():
         if world > 1:
             dist.barrier()
 
-    structures, log2s, seeds = make_structures(args.structures, MASTER_SEED + rank)
+    # one job: args.structures structures per GPU, made by one generator; with N GPUs the
+    # N * args.structures structures are shared out by LPT and one all-reduce of the block
+    # integers closes every step (at N = 1 there is nothing to exchange)
+    from ehss_b200.distributed import ShardedBatch
+    all_structures, all_log2s, all_seeds = make_structures(args.structures * world, MASTER_SEED)
+    job = ShardedBatch(all_structures, all_log2s, all_seeds, rank, world, repeats=REPEATS, cap=CAP,
+                       precision='fp32', graph=False) if world > 1 else None
+    if job is not None:
+        structures = [all_structures[i] for i in job.mine]
+        log2s = [all_log2s[i] for i in job.mine]
+        seeds = [all_seeds[i] for i in job.mine]
+        del job.batch            # rebuilt below with the tuned launch
+    else:
+        structures, log2s, seeds = all_structures, all_log2s, all_seeds
     launch = None
     if not args.no_autotune:
         from ehss_b200 import autotune
@@ -489,6 +505,12 @@ def main():
         launch, _ = autotune.tune(probe.plan.jobs, passes=1)
         del probe
     bc = BatchCCS(structures, log2s, seeds, repeats=REPEATS, cap=CAP, precision='fp32', launch=launch)
+    if job is not None:
+        job.batch = bc
+
+    def exchange():
+        if job is not None:
+            job.exchange()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
     stream = torch.cuda.current_stream()
 
@@ -496,6 +518,7 @@ def main():
     for _ in range(max(args.warmup, 3)):
         bc.build()
         bc.trace()
+        exchange()
     bc.run()
     torch.cuda.synchronize()
     # a long-running service moves its start-up objects out of the collector's
@@ -516,8 +539,11 @@ def main():
         e1.record(stream)
         bc.trace()
         e2.record(stream)
-        e2.synchronize()
-        step_ms.append(e0.elapsed_time(e2)); trace_ms.append(e1.elapsed_time(e2))
+        exchange()
+        e3 = torch.cuda.Event(enable_timing=True)
+        e3.record(stream)
+        e3.synchronize()
+        step_ms.append(e0.elapsed_time(e3)); trace_ms.append(e1.elapsed_time(e2))
     torch.cuda.synchronize(); barrier()
     clocks = sampler.stop()
     total_ms = float(sum(step_ms))
@@ -526,7 +552,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     rays_step = bc.rays
-    value = rays_step * world * args.steps / (total_ms * 1e-3)
+    job_rays = job.rays if job is not None else rays_step
+    value = job_rays * args.steps / (total_ms * 1e-3)
     structs_per_s = args.structures * world * args.steps / (total_ms * 1e-3)
     mean_trace_ms = float(np.mean(trace_ms))
     stats = np.sum([r['stats'] for r in bc.plan.collect()], axis=0)
@@ -535,6 +562,7 @@ def main():
     bc.plan.enqueue()
     cstats = np.sum([r['stats'] for r in bc.plan.collect()], axis=0)
     bc.plan.launch.options &= ~_lib.LAUNCH_COUNT_TESTS
+    bc.plan.enqueue()            # the block results of the timed work again (the checks below read them)
     own = {"box_tests_per_query": float(cstats[_lib.STAT_BOX]) / max(1, cstats[_lib.STAT_QUERIES]),
            "sphere_tests_per_query": float(cstats[_lib.STAT_SPHERE]) / max(1, cstats[_lib.STAT_QUERIES]),
            "queries_per_ray": float(cstats[_lib.STAT_QUERIES]) / rays_step}
@@ -547,6 +575,8 @@ def main():
         a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
         results = bc.run()
+        if job is not None:
+            job.exchange().cpu()     # the whole job's block integers on every rank's host
         b.record(stream)
         b.synchronize()
         e2e_ms.append(a.elapsed_time(b))
@@ -555,11 +585,11 @@ def main():
         t = torch.tensor([e2e_total], device='cuda', dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e_value = rays_step * world / (e2e_total * 1e-3)
+    e2e_value = job_rays / (e2e_total * 1e-3)
 
     # -- plain path: one structure per build + launch, no graph --------------------
     plain = None
-    if not args.no_plain:
+    if not args.no_plain and world == 1:
         from ehss_b200.blocks import BlockJob
         lib = _lib.load()
         import ctypes as ct
@@ -648,8 +678,9 @@ def main():
                "structure_rel_err_max": float(per_struct[full].max()) if full.any() else None,
                "oracle_seconds": check['seconds'], "oracle_threads": check['cores'],
                "rays": "the timed blocks' own device rays (same structures, seeds and 2^k counts)"}
-        configs = configuration_lines(eb, flush, peak_tflops)
-        explicit = explicit_trace_e2e(eb)
+        if world == 1:
+            configs = configuration_lines(eb, flush, peak_tflops)
+            explicit = explicit_trace_e2e(eb)
         if world == 1 and not args.no_cpu_baseline:
             rate, kind, cores, rays_done, secs = cpu_reference_rate(structures[::16], 12, 190003)
             cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
@@ -668,10 +699,11 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": config(args, world),
                 "structures_per_s": structs_per_s,
-                "rays_per_step": rays_step * world,
+                "rays_per_step": job_rays,
                 "trace_ms_per_step": mean_trace_ms, "build_ms_per_step": float(np.mean(step_ms) - mean_trace_ms),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bc.h2d_bytes,
-                        "d2h_bytes_per_step": bc.d2h_bytes, "ms_per_step": e2e_total,
+                        "d2h_bytes_per_step": bc.d2h_bytes + (job.packed.numel() * 8 if job is not None else 0),
+                        "ms_per_step": e2e_total,
                         "structures_per_s": args.structures * world / (e2e_total * 1e-3)},
                 "plain": plain,
                 "batched_over_plain": (value / world / plain['rays_per_s']) if plain else None,

@@ -93,6 +93,7 @@ _SIGNATURES = {
     'ehss_blocks_workspace_bytes': (ct.c_int, [ct.c_int, P]),
     'ehss_trace_blocks': (ct.c_int, [P, ct.c_int, I64, P, P, P, I64, P, U64, P, P]),
     'ehss_trace_blocks_residual': (ct.c_int, [P, ct.c_int, I64, P, P, P, I64, P, U64, P, P, I64, P, P]),
+    'ehss_trace_blocks_window': (ct.c_int, [P, ct.c_int, I64, I64, I64, P, P, P, I64, P, U64, P, P]),
     'ehss_extend_blocks': (ct.c_int, [P, ct.c_int, P, ct.c_int, P, I64, ct.c_int, P, P, P, P, I64, P, P, P]),
 }
 

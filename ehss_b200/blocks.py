@@ -129,6 +129,8 @@ class BlockPlan:
         total = ct.c_int64()
         _lib.check(lib.ehss_blocks_prepare(host, n, seeds, self.launch.chunk_rays, ct.byref(total)), 'blocks')
         self.total_chunks = total.value
+        self.chunk_begin = [int(host[i].chunk_begin) for i in range(n)]
+        self.window = None          # (first, end): trace only these chunks (one GPU's share)
         self.hist_entries = offset
         # descriptors through pinned memory: the upload does not wait for earlier work on the stream
         self._blocks_host = t.empty(ct.sizeof(host), dtype=t.uint8,
@@ -172,7 +174,15 @@ class BlockPlan:
         """Enqueue the launch on the current (or given) CUDA stream."""
         lib = _lib.load()
         s = stream_handle(self.device) if stream is None else stream
-        if self.residual is None:
+        if self.window is not None:
+            if self.residual is not None:
+                raise ValueError('a chunk window traces part of each block: no residual rays are saved')
+            first, end = self.window
+            _lib.check(lib.ehss_trace_blocks_window(ptr(self.blocks_dev), len(self.jobs), self.total_chunks, int(first),
+                                                    int(end), ptr(self.results), ptr(self.hist), ptr(self.ledger),
+                                                    self.hist_entries, ptr(self.work), self.work.numel() * 8,
+                                                    ct.byref(self.launch), s), 'trace blocks (window)')
+        elif self.residual is None:
             _lib.check(lib.ehss_trace_blocks(ptr(self.blocks_dev), len(self.jobs), self.total_chunks,
                                              ptr(self.results), ptr(self.hist), ptr(self.ledger), self.hist_entries,
                                              ptr(self.work), self.work.numel() * 8, ct.byref(self.launch), s),
@@ -184,6 +194,18 @@ class BlockPlan:
                                                       ct.byref(self.launch), ptr(self.residual),
                                                       self.residual_capacity, ptr(self.residual_count), s),
                        'trace blocks')
+
+    def chunk_costs(self):
+        """Estimated cost of every chunk (rays x (1 + log2 atoms) of its block),
+        in chunk order: the weights for cutting the chunk list into windows."""
+        out = np.zeros(self.total_chunks)
+        cr = self.launch.chunk_rays
+        for j, begin in zip(self.jobs, self.chunk_begin):
+            n = 1 << j.log2_rays
+            k = -(-n // cr)
+            per_ray = 1.0 + math.log2(max(2, int(j.scene.n_atoms)))
+            out[begin:begin + k] = per_ray * np.minimum(cr, n - cr * np.arange(k))
+        return out
 
     def capture(self):
         """Record the launch (resets + persistent kernel) in a CUDA graph."""

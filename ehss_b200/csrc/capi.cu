@@ -358,9 +358,16 @@ static int trace_blocks_impl(const ehss_block* blocks_dev, int n_blocks, int64_t
                              ehss_block_result* results_dev, uint64_t* hist_dev, uint64_t* ledger_dev,
                              int64_t hist_entries, void* workspace_dev, uint64_t workspace_bytes,
                              const ehss_launch* launch, ehss_residual* residual_dev, int64_t residual_capacity,
-                             unsigned long long* residual_count_dev, void* stream) {
+                             unsigned long long* residual_count_dev, void* stream, int64_t chunk_first = 0,
+                             int64_t chunk_end = -1) {
     if (!blocks_dev || n_blocks < 1 || !results_dev || !hist_dev || !ledger_dev || !workspace_dev || !launch) {
         set_error("invalid arguments");
+        return EHSS_ERR_VALUE;
+    }
+    if (chunk_end < 0) chunk_end = total_chunks;
+    if (total_chunks < 0 || chunk_first < 0 || chunk_first > chunk_end || chunk_end > total_chunks) {
+        set_error("chunk window [%lld, %lld) outside the %lld prepared chunks", (long long)chunk_first,
+                  (long long)chunk_end, (long long)total_chunks);
         return EHSS_ERR_VALUE;
     }
     if (workspace_bytes < sizeof(unsigned long long) * kMaxWorkParts) {
@@ -395,8 +402,8 @@ static int trace_blocks_impl(const ehss_block* blocks_dev, int n_blocks, int64_t
         rc = cuda_status(cudaMemsetAsync(residual_count_dev, 0, sizeof(unsigned long long), s), "residual count reset");
         if (rc) return rc;
     }
-    if (total_chunks == 0) return EHSS_OK;
-    return launch_blocks(blocks_dev, n_blocks, total_chunks, L, results_dev, hist_dev, ledger_dev,
+    if (chunk_end == chunk_first) return EHSS_OK;
+    return launch_blocks(blocks_dev, n_blocks, chunk_first, chunk_end - chunk_first, L, results_dev, hist_dev, ledger_dev,
                          reinterpret_cast<unsigned long long*>(workspace_dev), s, residual_dev, residual_capacity,
                          residual_count_dev);
 }
@@ -407,6 +414,16 @@ int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_
     clear_error();
     return trace_blocks_impl(blocks_dev, n_blocks, total_chunks, results_dev, hist_dev, ledger_dev, hist_entries,
                              workspace_dev, workspace_bytes, launch, nullptr, 0, nullptr, stream);
+}
+
+int ehss_trace_blocks_window(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks, int64_t chunk_first,
+                             int64_t chunk_end, ehss_block_result* results_dev, uint64_t* hist_dev,
+                             uint64_t* ledger_dev, int64_t hist_entries, void* workspace_dev, uint64_t workspace_bytes,
+                             const ehss_launch* launch, void* stream) {
+    clear_error();
+    return trace_blocks_impl(blocks_dev, n_blocks, total_chunks, results_dev, hist_dev, ledger_dev, hist_entries,
+                             workspace_dev, workspace_bytes, launch, nullptr, 0, nullptr, stream, chunk_first,
+                             chunk_end);
 }
 
 int ehss_trace_blocks_residual(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks,

@@ -254,7 +254,7 @@ int launch_extend(const ehss_block* blocks, int nb, const int32_t* row, int rows
                   int64_t n_in, int new_cap, ehss_extension* ext, uint64_t* hist, uint64_t* ledger,
                   ehss_residual* out, int64_t out_capacity, unsigned long long* out_count, uint64_t* stats,
                   cudaStream_t stream);
-int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const ehss_launch& L,
+int launch_blocks(const ehss_block* blocks, int nb, int64_t chunk_first, int64_t total_chunks, const ehss_launch& L,
                   ehss_block_result* results, uint64_t* hist, uint64_t* ledger, unsigned long long* work,
                   cudaStream_t stream, ehss_residual* residual = nullptr, int64_t residual_capacity = 0,
                   unsigned long long* residual_count = nullptr);

@@ -661,8 +661,10 @@ __device__ __noinline__ void save_residual(ehss_residual* residual, long long ca
 // structure, and neighbouring regions of its ray space, at the same time and
 // share their L1.  A warp whose range is used up takes chunks from the next
 // ranges in turn.  counters[p] counts the chunks handed out from range p.
-__device__ __forceinline__ bool next_chunk(unsigned long long* counters, int n_parts, int& scan, int64_t total,
-                                           long long& chunk) {
+// Only the window [first, first + total) of the chunk list is traced (the
+// whole list, or one GPU's share of it).
+__device__ __forceinline__ bool next_chunk(unsigned long long* counters, int n_parts, int& scan, int64_t first,
+                                           int64_t total, long long& chunk) {
     for (; scan < n_parts; ++scan) {
         unsigned smid;
         asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
@@ -670,7 +672,7 @@ __device__ __forceinline__ bool next_chunk(unsigned long long* counters, int n_p
         int64_t begin = total * p / n_parts, end = total * (p + 1) / n_parts;
         if (begin >= end) continue;
         unsigned long long t = atomicAdd(counters + p, 1ull);
-        if (begin + (int64_t)t < end) { chunk = begin + (int64_t)t; return true; }
+        if (begin + (int64_t)t < end) { chunk = first + begin + (int64_t)t; return true; }
     }
     return false;
 }
@@ -678,8 +680,9 @@ __device__ __forceinline__ bool next_chunk(unsigned long long* counters, int n_p
 // RAYS: the instance for blocks with EHSS_BLOCK_RAYS (caller-made weighted rays);
 // each instance skips the other kind's chunks, like the precision instances.
 template <bool EXACT, bool COUNT, bool RAYS>
-__global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int nb, int64_t total_chunks,
-                                                   int chunk_rays, int resolve_batch, ehss_block_result* results,
+__global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int nb, int64_t chunk_first,
+                                                   int64_t total_chunks, int chunk_rays, int resolve_batch,
+                                                   ehss_block_result* results,
                                                    uint64_t* hist, uint64_t* ledger, unsigned long long* work,
                                                    int n_parts, int smem_stack, ehss_residual* residual,
                                                    long long residual_capacity, unsigned long long* residual_count) {
@@ -699,7 +702,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
     while (true) {
         long long c = 0;
         int have = 0;
-        if (lane == 0) have = next_chunk(work, n_parts, scan, total_chunks, c);
+        if (lane == 0) have = next_chunk(work, n_parts, scan, chunk_first, total_chunks, c);
         have = __shfl_sync(0xffffffffu, have, 0);
         if (!have) break;
         c = __shfl_sync(0xffffffffu, c, 0);
@@ -945,7 +948,7 @@ int launch_source_rays(const void* scene, const Sobol4Params& p, int64_t first, 
     return cuda_status(cudaGetLastError(), "source launch");
 }
 
-int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const ehss_launch& L,
+int launch_blocks(const ehss_block* blocks, int nb, int64_t chunk_first, int64_t total_chunks, const ehss_launch& L,
                   ehss_block_result* results, uint64_t* hist, uint64_t* ledger, unsigned long long* work,
                   cudaStream_t stream, ehss_residual* residual, int64_t residual_capacity,
                   unsigned long long* residual_count) {
@@ -974,7 +977,7 @@ int launch_blocks(const ehss_block* blocks, int nb, int64_t total_chunks, const 
             const int n_parts = sm_count() < kMaxWorkParts ? sm_count() : kMaxWorkParts;
 #define EHSS_LAUNCH_BLOCKS(E, C, R) \
             k_blocks<E, C, R><<<grid, L.block_threads, R ? smem_rays : smem, stream>>>( \
-                blocks, nb, total_chunks, L.chunk_rays, batch, results, hist, ledger, work, n_parts, sdepth, \
+                blocks, nb, chunk_first, total_chunks, L.chunk_rays, batch, results, hist, ledger, work, n_parts, sdepth, \
                 residual, residual_capacity, residual_count)
             if (exact) {
                 if (rays) { if (count) EHSS_LAUNCH_BLOCKS(true, true, true); else EHSS_LAUNCH_BLOCKS(true, false, true); }

@@ -333,6 +333,19 @@ int ehss_trace_blocks(const ehss_block* blocks_dev, int n_blocks, int64_t total_
                       int64_t hist_entries, void* workspace_dev, uint64_t workspace_bytes,
                       const ehss_launch* launch, void* stream);
 
+/* ehss_trace_blocks over the window [chunk_first, chunk_end) of the prepared
+ * chunk list only (0 <= chunk_first <= chunk_end <= total_chunks): the
+ * several-GPU form of one batch.  Each GPU traces a disjoint window of the
+ * same blocks; its results/hist/ledger hold the integer sums of its rays, and
+ * the element-wise sum over GPUs equals the single-launch results exactly.
+ * Replaces the reference's parallel loop over the rays of one structure
+ * (prange, src/support_exchange_transport/ehss_cpu.py:72; OpenMP,
+ * src/native/ehss_cpu.cpp:49-53) at the scale of several devices. */
+int ehss_trace_blocks_window(const ehss_block* blocks_dev, int n_blocks, int64_t total_chunks, int64_t chunk_first,
+                             int64_t chunk_end, ehss_block_result* results_dev, uint64_t* hist_dev,
+                             uint64_t* ledger_dev, int64_t hist_entries, void* workspace_dev, uint64_t workspace_bytes,
+                             const ehss_launch* launch, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Cap extension.  The reference's production runs start at cap 512 and
  * retrace the same rays at caps 1024, 2048 and 4096 while a run's sampled

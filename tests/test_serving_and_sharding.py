@@ -185,3 +185,83 @@ def test_sharded_gather_with_two_gloo_ranks():
         assert p.exitcode == 0
     assert [r['structure'] for r in res] == list(range(len(structures)))
     assert [r['value'] for r in res] == [float(len(s[1]) * 2 + i) for i, s in enumerate(structures)]
+
+
+def test_chunk_windows_cover_the_list_by_cost():
+    rng = np.random.default_rng(3)
+    for n, world in [(0, 2), (1, 3), (10, 3), (1000, 8), (5, 8)]:
+        costs = rng.uniform(0.5, 20.0, n)
+        w = D.chunk_windows(costs, world)
+        assert len(w) == world and w[0][0] == 0 and w[-1][1] == n
+        assert all(a[1] == b[0] for a, b in zip(w, w[1:])) and all(f <= e for f, e in w)
+        if n >= 100:
+            loads = [costs[f:e].sum() for f, e in w]
+            assert max(loads) - min(loads) <= 2 * costs.max()
+
+
+def test_global_index_partitions_the_batch_layout():
+    S, R, W, H1 = 7, 3, 16, 9
+    owner = D.shard([D.estimated_cost(n, 1 << 14) for n in (20, 300, 5000, 45, 1200, 7, 90)], 3)
+    parts = [D.global_index([i for i, o in enumerate(owner) if o == r], S, R, W, H1) for r in range(3)]
+    allidx = np.concatenate(parts)
+    assert len(allidx) == S * R * W + 2 * S * R * H1
+    np.testing.assert_array_equal(np.sort(allidx), np.arange(len(allidx)))
+    # a rank holding every structure in order has the global layout itself
+    np.testing.assert_array_equal(D.global_index(list(range(S)), S, R, W, H1), np.arange(len(allidx)))
+
+
+class _FakeWindowPlan:
+    """A plan whose 'kernel' sums integer functions of its rays: chunk c holds
+    rays [c*8, c*8 + 8) of one of three blocks; packed = per-block sums."""
+
+    def __init__(self):
+        import torch
+        self.blocks = [(0, 5), (5, 12), (12, 13)]      # chunk ranges of three blocks
+        self.total_chunks = 13
+        self.window = None
+        self.packed = torch.zeros(6, dtype=torch.int64)
+
+    def chunk_costs(self):
+        return [1.0 + (c % 4) for c in range(self.total_chunks)]
+
+    def enqueue(self):
+        first, end = self.window if self.window is not None else (0, self.total_chunks)
+        self.packed.zero_()
+        for b, (lo, hi) in enumerate(self.blocks):
+            for c in range(max(lo, first), min(hi, end)):
+                for ray in range(c * 8, c * 8 + 8):
+                    self.packed[2 * b] += (ray * 2654435761) % 1000003     # a fixed-point 'angle'
+                    self.packed[2 * b + 1] += ray % 3 == 0                   # a count
+
+
+def _window_worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        plan = _FakeWindowPlan()
+        windows = D.trace_window_split(plan, rank, world)
+        out.put((rank, windows, plan.packed.tolist()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_window_split_sums_equal_one_rank_with_two_gloo_ranks():
+    import torch.multiprocessing as mp
+    whole = _FakeWindowPlan()
+    whole.enqueue()
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_window_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, windows, packed in got:
+        assert windows[0][0] == 0 and windows[-1][1] == 13 and windows[0][1] == windows[1][0]
+        assert packed == whole.packed.tolist()      # every rank holds the whole plan's integers
