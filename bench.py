@@ -221,6 +221,45 @@ def cpu_reference_rate(structures, log2, seed, budget_s=12.0, threads=None):
     return rays / elapsed, kind, threads, rays, elapsed
 
 
+def numba_reference_rates(structures, log2, seed, budget_s=5.0):
+    """The reference's production kernel, ``PreparedStaticCPUEHSS(spheres,
+    threads=T).engine.trace(source, cap)`` (Numba; ehss_cpu.py:118-142), run
+    from the reference package installed into baseline/_ref, on the same
+    sample as the C++ baseline: T = 1 and T = every host thread.  Sources
+    (the reference's external_source) and JIT compilation stay outside the
+    timing, as the reference CLI times them apart."""
+    ref = ROOT / 'baseline' / '_ref'
+    if not (ref / 'support_exchange_transport').is_dir():
+        return {"unavailable": "the reference package is not installed in baseline/_ref"}
+    sys.path.insert(0, str(ref))
+    try:
+        import numba
+        from support_exchange_transport.ehss_state import external_source
+        from support_exchange_transport.ehss_static import PreparedStaticCPUEHSS
+        from support_exchange_transport.inside_out_pa import Spheres
+    except Exception as exc:          # noqa: BLE001 - report why the arm is missing
+        return {"unavailable": f"{type(exc).__name__}: {exc}"}
+    cores = int(numba.config.NUMBA_NUM_THREADS)
+    work = []
+    for c, r in structures:
+        s = Spheres(np.asarray(c, dtype=np.float64), np.asarray(r, dtype=np.float64), deduplicate=False)
+        work.append((s, external_source(s, log2, seed)))
+    out = {"kind": "reference (Numba CPUEHSSTransport.trace)", "unit": UNIT,
+           "sample": f"{len(structures)} structures, 2^{log2} rays each, cap {CAP}, trace only"}
+    for threads in sorted({1, cores}):
+        engines = [(PreparedStaticCPUEHSS(s, threads=threads).engine, src) for s, src in work]
+        engines[0][0].trace(engines[0][1], CAP)            # JIT compilation
+        rays, elapsed = 0, 0.0
+        while elapsed < budget_s or rays == 0:
+            for eng, src in engines:
+                t0 = time.perf_counter()
+                eng.trace(src, CAP)
+                elapsed += time.perf_counter() - t0
+                rays += len(src.weights)
+        out[f"threads_{threads}"] = {"value": rays / elapsed, "cores": threads, "rays": rays, "seconds": elapsed}
+    return out
+
+
 def configuration_lines(eb, flush, peak_of, reps=10):
     """The single-structure configurations, each as one persistent launch of
     its seed blocks (exterior scene, cap 64), timed with CUDA events after an
@@ -685,7 +724,8 @@ def main():
             rate, kind, cores, rays_done, secs = cpu_reference_rate(structures[::16], 12, 190003)
             cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
                    "sample": f"{len(structures[::16])} of {len(structures)} structures (every 16th), 2^12 rays each, "
-                             f"cap {CAP}; {rays_done} rays in {secs:.1f} s"}
+                             f"cap {CAP}; {rays_done} rays in {secs:.1f} s",
+                   "numba": numba_reference_rates(structures[::16], 12, 190003)}
     serve = None
     if rank == 0 and world == 1 and not args.no_serve:
         serve = serving_measurement()

@@ -287,14 +287,15 @@ class BlockPlan:
                                                       _lib.STAT_FALLBACK, _lib.STAT_QUERIES))
         out = []
         for i, j in enumerate(self.jobs):
-            d = {'tag': j.tag, 'rays': 1 << j.log2_rays, 'weight': wl[i], 'radius': self._radius[i], 'stats': stats[i]}
+            d = {'tag': j.tag, 'rays': 1 << j.log2_rays, 'weight': wl[i], 'radius': self._radius[i], 'stats': stats[i],
+                 'sphere_tests': sph[i], 'box_tests': box[i]}
             if j.ehss:
                 o = self._offsets[i]
                 e = o + j.cap + 1
                 d.update({'ehss_angstrom2': ehss[i], 'pa_from_same_rays_angstrom2': pa_same[i],
                           'tail_bound_angstrom2': tail[i], 'unresolved_rays': unres[i], 'escaped_rays': esc[i],
                           'collision_histogram': hist[o:e], 'collision_contribution_angstrom2': ledger[o:e],
-                          'sphere_tests': sph[i], 'box_tests': box[i], 'grazing_queries': graz[i],
+                          'grazing_queries': graz[i],
                           'fp64_fallback_queries': fall[i], 'queries': qry[i]})
             if j.pa:
                 d['pa_angstrom2'] = pa_area[i]

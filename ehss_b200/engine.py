@@ -161,7 +161,16 @@ def external_source(spheres, power, seed, scene=None):
 
 
 class GPUEHSSTransport:
-    """EHSS tracer on one prepared scene (CPUEHSSTransport.trace contract)."""
+    """EHSS tracer on one prepared scene (CPUEHSSTransport.trace contract).
+
+    ``trace`` takes and returns host arrays, as the reference does.  The rays
+    go through in up to four chunks on two streams, so one chunk's copy to
+    the device overlaps the previous chunk's trace and copy back; results are
+    copied into page-locked host buffers that become the returned arrays (no
+    second copy).  Device buffers are kept and grown across calls.
+    """
+
+    PIPELINE_MIN_CHUNK = 1 << 15
 
     def __init__(self, scene, precision='fp32', threads=1):
         if getattr(scene, 'exterior', False):
@@ -169,6 +178,22 @@ class GPUEHSSTransport:
         self.scene = scene
         self.precision = _precision(precision)
         self.threads = threads
+        self._dev = None
+        self._dev_rays = 0
+        self._streams = None
+
+    def _buffers(self, n, cap, record_history):
+        t = torch()
+        dev = self.scene.device
+        if self._dev is None or self._dev_rays < n:
+            self._dev = dict(P=t.empty((n, 3), dtype=t.float64, device=dev), D=t.empty((n, 3), dtype=t.float64, device=dev),
+                             last=t.empty(n, dtype=t.int64, device=dev), bounces=t.empty(n, dtype=t.int64, device=dev),
+                             esc=t.empty(n, dtype=t.uint8, device=dev), unres=t.empty(n, dtype=t.uint8, device=dev))
+            self._dev_rays = n
+        if self._streams is None:
+            self._streams = [t.cuda.Stream(dev), t.cuda.Stream(dev)]
+        hist = t.empty((n, cap), dtype=t.int32, device=dev) if record_history else None
+        return self._dev, hist
 
     def trace(self, source, cap=64, record_history=False):
         if type(cap) is not int or cap < 1 or cap > np.iinfo(np.int32).max or np.any(source.initial_bounces > 1):
@@ -178,25 +203,53 @@ class GPUEHSSTransport:
             raise ValueError('Invalid initial physical identity')
         lib = _lib.load()
         t = torch()
-        dev = self.scene.device
         start = time.perf_counter()
         n = len(source.weights)
-        P = to_device(source.origins, np.float64, dev)
-        D = to_device(source.directions, np.float64, dev)
-        last = to_device(source.last_atom, np.int64, dev)
-        bounces = to_device(source.initial_bounces, np.int64, dev)
-        esc = t.zeros(n, dtype=t.uint8, device=dev)
-        unres = t.zeros(n, dtype=t.uint8, device=dev)
-        hist = t.full((n, cap), -1, dtype=t.int32, device=dev) if record_history else None
-        stats = t.zeros(_lib.NSTATS, dtype=t.int64, device=dev)
-        _lib.check(lib.ehss_trace(self.scene.ptr, n, cap, self.precision, ptr(P), ptr(D), ptr(last), ptr(bounces),
-                                  ptr(esc), ptr(unres), ptr(hist), ptr(stats), stream_handle(dev)), 'trace')
-        st = stats.cpu().numpy().astype(np.uint64)
+        # host inputs as tensors over the caller's memory (no copy when already contiguous of the right type)
+        host_in = dict(P=t.from_numpy(np.ascontiguousarray(source.origins, dtype=np.float64)),
+                       D=t.from_numpy(np.ascontiguousarray(source.directions, dtype=np.float64)),
+                       last=t.from_numpy(np.ascontiguousarray(source.last_atom, dtype=np.int64)),
+                       bounces=t.from_numpy(np.ascontiguousarray(source.initial_bounces, dtype=np.int64)))
+        d, hist = self._buffers(max(n, 1), cap, record_history)
+        # results land in page-locked buffers that become the returned arrays
+        pin = dict(pin_memory=True)
+        out = dict(P=t.empty((n, 3), dtype=t.float64, **pin), D=t.empty((n, 3), dtype=t.float64, **pin),
+                   bounces=t.empty(n, dtype=t.int64, **pin), esc=t.empty(n, dtype=t.uint8, **pin),
+                   unres=t.empty(n, dtype=t.uint8, **pin))
+        hist_out = t.empty((n, cap), dtype=t.int32, **pin) if record_history else None
+        stats = t.zeros(_lib.NSTATS, dtype=t.int64, device=self.scene.device)
+        main = t.cuda.current_stream(self.scene.device)
+        parts = max(1, min(4, n // self.PIPELINE_MIN_CHUNK))
+        bounds = [n * k // parts for k in range(parts + 1)]
+        for s in self._streams:
+            s.wait_stream(main)           # stats zeroed, buffers free
+        for k in range(parts):
+            a, b = bounds[k], bounds[k + 1]
+            if a == b:
+                continue
+            s = self._streams[k % 2]
+            with t.cuda.stream(s):
+                for key in ('P', 'D', 'last', 'bounces'):
+                    d[key][a:b].copy_(host_in[key][a:b], non_blocking=True)
+                if hist is not None:
+                    hist[a:b].fill_(-1)
+                _lib.check(lib.ehss_trace(self.scene.ptr, b - a, cap, self.precision, ptr(d['P'][a:b]),
+                                          ptr(d['D'][a:b]), ptr(d['last'][a:b]), ptr(d['bounces'][a:b]),
+                                          ptr(d['esc'][a:b]), ptr(d['unres'][a:b]),
+                                          None if hist is None else ptr(hist[a:b]), ptr(stats), s.cuda_stream),
+                           'trace')
+                for key in ('P', 'D', 'bounces', 'esc', 'unres'):
+                    out[key][a:b].copy_(d[key][a:b], non_blocking=True)
+                if hist is not None:
+                    hist_out[a:b].copy_(hist[a:b], non_blocking=True)
+        for s in self._streams:
+            main.wait_stream(s)
+        st = stats.cpu().numpy().astype(np.uint64)       # synchronises the main stream, hence both others
         if st[_lib.STAT_ERRORS]:
             raise _lib.EHSSDeviceError(f'{int(st[_lib.STAT_ERRORS])} rays reported a bounded device failure')
-        history = hist.cpu().numpy() if record_history else np.full((n, 0), -1, dtype=np.int32)
-        return EHSSResult(P.cpu().numpy(), D.cpu().numpy(), esc.cpu().numpy().astype(bool),
-                          unres.cpu().numpy().astype(bool), bounces.cpu().numpy(), history, source,
+        history = hist_out.numpy() if record_history else np.full((n, 0), -1, dtype=np.int32)
+        return EHSSResult(out['P'].numpy(), out['D'].numpy(), out['esc'].numpy().view(np.bool_),
+                          out['unres'].numpy().view(np.bool_), out['bounces'].numpy(), history, source,
                           dict(query_s=time.perf_counter() - start, sphere_tests=int(st[_lib.STAT_SPHERE]),
                                box_tests=int(st[_lib.STAT_BOX]), queries=int(st[_lib.STAT_QUERIES]),
                                grazing_queries=int(st[_lib.STAT_GRAZING]),
