@@ -5,7 +5,12 @@ computes) must equal one launch of the whole job bit for bit.
 
 * ray windows: one 2000-atom structure's 20 seed blocks (the precision
   configuration's shape at 2^14 rays per seed) cut into 3 and 8 windows;
-* structure shards: a 24-structure mixed batch over 3 ranks."""
+* structure shards: a 24-structure mixed batch over 3 ranks.  A shard's
+  plan has fewer rays, so it takes smaller chunks; a lane's traversal order
+  depends on its warp-mates (leaves are postponed until the warp's lanes
+  all hold one), so the diagnostic counters of tests made (box, sphere,
+  FP64 re-tests, grazing and fallback queries) can differ, while every
+  outcome integer and the per-ray query and error counts are equal."""
 import numpy as np
 import pytest
 
@@ -69,4 +74,11 @@ def test_structure_shards_add_up_to_one_batch(eb):
         part.trace()
         total += part.scatter()
     assert sorted(i for m in owners for i in m) == list(range(24))
-    assert bool((total == ref).all())
+    from ehss_b200 import _lib
+    from ehss_b200.blocks import _RESULT_WORDS, _STATS0
+    n_res = 24 * 3 * _RESULT_WORDS
+    words = np.arange(n_res) % _RESULT_WORDS
+    order_free = (words < _STATS0) | (words == _STATS0 + _lib.STAT_QUERIES) | (words == _STATS0 + _lib.STAT_ERRORS)
+    a, b = total.cpu().numpy(), ref.cpu().numpy()
+    np.testing.assert_array_equal(a[:n_res][order_free], b[:n_res][order_free])
+    np.testing.assert_array_equal(a[n_res:], b[n_res:])          # histograms and ledgers
