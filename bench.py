@@ -526,7 +526,17 @@ def main():
     # N * args.structures structures are shared out by LPT and one all-reduce of the block
     # integers closes every step (at N = 1 there is nothing to exchange)
     from ehss_b200.distributed import ShardedBatch
-    all_structures, all_log2s, all_seeds = make_structures(args.structures * world, MASTER_SEED)
+    if world > 1:
+        # every rank makes only its own structures (the LPT shares follow from the sizes alone)
+        from ehss_b200 import distributed as D, workloads as W
+        spec = W.mixed_batch(args.structures * world, seed=MASTER_SEED)
+        owner = D.shard([D.estimated_cost(n, 1 << lg) for n, lg, _ in spec], world)
+        all_structures = [W.globule(n, sd)[:2] if o == rank else (np.zeros((n, 3)), np.ones(n))
+                          for (n, _, sd), o in zip(spec, owner)]
+        all_log2s = [lg for _, lg, _ in spec]
+        all_seeds = [sd % (2 ** 32) for _, _, sd in spec]
+    else:
+        all_structures, all_log2s, all_seeds = make_structures(args.structures, MASTER_SEED)
     job = ShardedBatch(all_structures, all_log2s, all_seeds, rank, world, repeats=REPEATS, cap=CAP,
                        precision='fp32', graph=False) if world > 1 else None
     if job is not None:
