@@ -116,7 +116,8 @@ class ShardedBatch:
     histogram and ledger entries per block) and sums it over the ranks, so
     every rank ends with every block's totals."""
 
-    def __init__(self, structures, log2s, seeds, rank, world, group=None, repeats=3, cap=64, **batch_kw):
+    def __init__(self, structures, log2s, seeds, rank, world, group=None, repeats=3, cap=64, batch_factory=None,
+                 **batch_kw):
         from .blocks import _RESULT_WORDS
         from .device import torch
         t = torch()
@@ -129,9 +130,10 @@ class ShardedBatch:
         S, R, H1, W = len(structures), self.repeats, self.cap + 1, _RESULT_WORDS
         self.batch = None
         if self.mine:
-            from .batch import BatchCCS
-            self.batch = BatchCCS([structures[i] for i in self.mine], [log2s[i] for i in self.mine],
-                                  [seeds[i] for i in self.mine], repeats=repeats, cap=cap, **batch_kw)
+            if batch_factory is None:
+                from .batch import BatchCCS as batch_factory
+            self.batch = batch_factory([structures[i] for i in self.mine], [log2s[i] for i in self.mine],
+                                       [seeds[i] for i in self.mine], repeats=repeats, cap=cap, **batch_kw)
             device = self.batch.device
         else:
             device = t.device('cuda', t.cuda.current_device()) if t.cuda.is_available() else t.device('cpu')

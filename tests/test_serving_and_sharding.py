@@ -265,3 +265,80 @@ def test_window_split_sums_equal_one_rank_with_two_gloo_ranks():
     for rank, windows, packed in got:
         assert windows[0][0] == 0 and windows[-1][1] == 13 and windows[0][1] == windows[1][0]
         assert packed == whole.packed.tolist()      # every rank holds the whole plan's integers
+
+
+class _FakeBatch:
+    """Stands in for BatchCCS on CPU: the packed block results are integers
+    that depend only on (structure, replicate), laid out as a BlockPlan lays
+    them out (result words per block, then histogram, then ledger entries)."""
+    W = 16
+
+    def __init__(self, structures, log2s, seeds, repeats=3, cap=64):
+        import torch
+        self.device = torch.device('cpu')
+        self.rays = sum((1 << lg) * repeats for lg in log2s)
+        ids = [int(np.round(c.sum() * 1000)) % 100003 for c, _ in structures]
+        n = len(structures) * repeats
+        res = np.array([[ids[b // repeats] * 7 + (b % repeats) * 3 + w for w in range(self.W)] for b in range(n)])
+        hist = np.array([[ids[b // repeats] + k + b % repeats for k in range(cap + 1)] for b in range(n)])
+        self.packed_np = np.concatenate([res.ravel(), hist.ravel(), 2 * hist.ravel()]).astype(np.int64)
+        self.plan = type('Plan', (), {})()
+        self.plan.packed = torch.from_numpy(self.packed_np.copy())
+
+    def upload(self):
+        pass
+
+    def build(self):
+        pass
+
+    def trace(self):
+        pass
+
+
+def _sharded_worker(rank, world, port, structures, log2s, seeds, out):
+    import torch.distributed as dist
+    from ehss_b200 import blocks
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        blocks._RESULT_WORDS = _FakeBatch.W
+        job = D.ShardedBatch(structures, log2s, seeds, rank, world, repeats=3, cap=8, batch_factory=_FakeBatch)
+        packed = job.step().clone()
+        out.put((rank, job.mine, packed.numpy().tolist()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_structure_shards_exchange_with_two_gloo_ranks():
+    """Each rank holds only its LPT share; after the all-reduce every rank's
+    buffer equals the one-rank layout of the whole batch."""
+    import torch.multiprocessing as mp
+    from ehss_b200 import blocks
+    rng = np.random.default_rng(5)
+    sizes = (20, 300, 5000, 45, 1200, 7, 90)
+    structures = [(rng.normal(size=(n, 3)), np.ones(n)) for n in sizes]
+    log2s, seeds = [14, 16, 18, 15, 17, 14, 16], [1, 2, 3, 4, 5, 6, 7]
+    saved = blocks._RESULT_WORDS
+    blocks._RESULT_WORDS = _FakeBatch.W
+    try:
+        whole = D.ShardedBatch(structures, log2s, seeds, 0, 1, repeats=3, cap=8, batch_factory=_FakeBatch)
+        ref = whole.step().numpy().tolist()
+    finally:
+        blocks._RESULT_WORDS = saved
+    assert ref == whole.batch.packed_np.tolist()
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sharded_worker, args=(r, 2, port, structures, log2s, seeds, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    mines = sorted(i for _, mine, _ in got for i in mine)
+    assert mines == list(range(len(sizes)))
+    for rank, mine, packed in got:
+        assert packed == ref, rank
