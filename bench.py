@@ -526,26 +526,22 @@ def main():
     # N * args.structures structures are shared out by LPT and one all-reduce of the block
     # integers closes every step (at N = 1 there is nothing to exchange)
     from ehss_b200.distributed import ShardedBatch
+    mine = None
     if world > 1:
         # every rank makes only its own structures (the LPT shares follow from the sizes alone)
         from ehss_b200 import distributed as D, workloads as W
         spec = W.mixed_batch(args.structures * world, seed=MASTER_SEED)
         owner = D.shard([D.estimated_cost(n, 1 << lg) for n, lg, _ in spec], world)
+        mine = [i for i, o in enumerate(owner) if o == rank]
         all_structures = [W.globule(n, sd)[:2] if o == rank else (np.zeros((n, 3)), np.ones(n))
                           for (n, _, sd), o in zip(spec, owner)]
         all_log2s = [lg for _, lg, _ in spec]
         all_seeds = [sd % (2 ** 32) for _, _, sd in spec]
+        structures = [all_structures[i] for i in mine]
+        log2s = [all_log2s[i] for i in mine]
+        seeds = [all_seeds[i] for i in mine]
     else:
-        all_structures, all_log2s, all_seeds = make_structures(args.structures, MASTER_SEED)
-    job = ShardedBatch(all_structures, all_log2s, all_seeds, rank, world, repeats=REPEATS, cap=CAP,
-                       precision='fp32', graph=False) if world > 1 else None
-    if job is not None:
-        structures = [all_structures[i] for i in job.mine]
-        log2s = [all_log2s[i] for i in job.mine]
-        seeds = [all_seeds[i] for i in job.mine]
-        del job.batch            # rebuilt below with the tuned launch
-    else:
-        structures, log2s, seeds = all_structures, all_log2s, all_seeds
+        structures, log2s, seeds = make_structures(args.structures, MASTER_SEED)
     launch = None
     if not args.no_autotune:
         from ehss_b200 import autotune
@@ -553,9 +549,14 @@ def main():
         probe.upload(); probe.build()
         launch, _ = autotune.tune(probe.plan.jobs, passes=1)
         del probe
-    bc = BatchCCS(structures, log2s, seeds, repeats=REPEATS, cap=CAP, precision='fp32', launch=launch)
-    if job is not None:
-        job.batch = bc
+    job = None
+    if world > 1:
+        job = ShardedBatch(all_structures, all_log2s, all_seeds, rank, world, repeats=REPEATS, cap=CAP,
+                           precision='fp32', launch=launch)
+        assert job.mine == mine
+        bc = job.batch
+    else:
+        bc = BatchCCS(structures, log2s, seeds, repeats=REPEATS, cap=CAP, precision='fp32', launch=launch)
 
     def exchange():
         if job is not None:
