@@ -363,7 +363,8 @@ def explicit_trace_e2e(eb, reps=5):
         res = prep.engine.trace(src, CAP)
         ms.append((time.perf_counter() - t0) * 1e3)
     n = len(src.weights)
-    return {"workload": "C3 rays (2000-atom globule, 2^18 rays, seed 0) through engine.trace with host arrays",
+    return {"workload": "C3 rays (2000-atom globule, 2^18 rays, seed 0) through engine.trace with host arrays "
+                        "(the source as external_source returns it: numpy arrays over page-locked memory)",
             "ms_per_call": float(np.median(ms)), "rays_per_s": n / (float(np.median(ms)) * 1e-3),
             "h2d_bytes_per_call": n * (24 + 24 + 8 + 8), "d2h_bytes_per_call": n * (24 + 24 + 1 + 1 + 8),
             "timer": "host clock around the synchronous call (median of %d)" % reps,

@@ -144,7 +144,9 @@ def external_source(spheres, power, seed, scene=None):
     """Impact-disk source generated on the device from bit-exact Sobol points.
 
     Same contract as the reference's external_source: 2**power rays, weight
-    pi R^2 / n each, no initial collider.
+    pi R^2 / n each, no initial collider.  The ray arrays are numpy arrays
+    over page-locked host memory, so handing them back to a trace copies them
+    to the device by DMA.
     """
     power = int(power)
     if not 0 <= power <= 30:
@@ -152,11 +154,17 @@ def external_source(spheres, power, seed, scene=None):
     seed = _check_seed(seed)
     scene = scene or Scene.from_spheres(spheres)
     o, d = scene.source_rays(power, seed)
-    origins = o.cpu().numpy()
-    directions = d.cpu().numpy()
+    t = torch()
+    # page-locked host arrays: the copy back and a later trace's copy in run as DMA
+    host = t.empty((3, o.shape[0], 3), dtype=t.float64, pin_memory=True)
+    host[0].copy_(o, non_blocking=True)
+    host[1].copy_(d, non_blocking=True)
+    host[2].copy_(d, non_blocking=True)
+    t.cuda.current_stream(scene.device).synchronize()
+    origins, directions, incoming = (a.numpy() for a in host)
     n = len(origins)
     R = scene.radius
-    return EHSSSource(origins, directions, directions.copy(), np.full(n, np.pi * R * R / n),
+    return EHSSSource(origins, directions, incoming, np.full(n, np.pi * R * R / n),
                       np.full(n, -1), np.zeros(n, dtype=np.int64), "external impact disk")
 
 
