@@ -69,6 +69,13 @@ def test_argument_validation_without_device(lib):
                                     1 << 20, 1, None) == _lib.ERR_VALUE
     with pytest.raises(ValueError):
         _lib.check(_lib.ERR_VALUE)
+    # a chunk window must lie inside the prepared chunk list (checked before any device work)
+    L = _lib.Launch(128, 8, 256, 28, 0, 0, 5, 0)
+    ws = (ct.c_uint64 * 512)()
+    for first, end in ((5, 3), (-1, 2), (0, 11)):
+        rc = lib.ehss_trace_blocks_window(ct.c_void_p(1024), 1, 10, first, end, ct.c_void_p(1024), ct.c_void_p(1024),
+                                          ct.c_void_p(1024), 1, ws, ct.sizeof(ws), ct.byref(L), None)
+        assert rc == _lib.ERR_VALUE and b'chunk window' in lib.ehss_last_error()
 
 
 def test_noalloc_limit_fits_the_fixed_scratch_array(lib):
