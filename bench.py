@@ -683,7 +683,7 @@ def main():
                  "latency_ms_p99": float(np.percentile(lats, 99))}
 
     # -- roofline, CPU baseline and CCS error (rank 0, N = 1 only for the baseline) ---
-    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    n_sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     clock_mhz = float(clocks['sm_mhz']) if clocks else 1965.0
 
     def peak_tflops():
