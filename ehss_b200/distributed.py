@@ -140,11 +140,13 @@ class ShardedBatch:
         # where each element of the local packed buffer goes in the global one
         self.global_words = S * R * W + 2 * S * R * H1
         idx = global_index(self.mine, S, R, W, H1)
-        if self.mine:
-            assert len(idx) == self.batch.plan.packed.numel()
+        if self.mine and len(idx) != self.batch.plan.packed.numel():
+            raise ValueError('every block of the batch must have the same cap (the global layout assumes cap + 1 '
+                             'histogram entries per block)')
         self.index = t.as_tensor(idx, device=device)
         self.packed = t.zeros(self.global_words, dtype=t.int64, device=device)
         self.rays = sum((1 << int(log2s[i])) * R for i in range(S))
+        self._structures, self._log2s = structures, [int(x) for x in log2s]
         self.local_rays = self.batch.rays if self.batch is not None else 0
 
     def upload(self):
@@ -177,3 +179,26 @@ class ShardedBatch:
         self.build()
         self.trace()
         return self.exchange()
+
+    def summaries(self):
+        """Every structure's EHSS over its replicates (mean, sd, sem), mean
+        tail bound and unresolved rays, from the exchanged integers: the same
+        numbers on every rank, and the same as one GPU's BatchCCS.  The block
+        weights need each structure's impact-disk radius, so every
+        structure's real coordinates must have been passed in."""
+        from . import _lib
+        from .batch import enclosing_radius, summarize
+        from .blocks import _RESULT_WORDS
+        S, R, W = self.n_structures, self.repeats, _RESULT_WORDS
+        packed = self.packed.cpu().numpy().view(np.uint64)
+        res = packed[:S * R * W].reshape(S * R, W)
+        out = []
+        for s, ((c, r), lg) in enumerate(zip(self._structures, self._log2s)):
+            radius = enclosing_radius(c, r)
+            w = np.pi * radius * radius / float(1 << lg)
+            rows = res[s * R:(s + 1) * R]
+            ehss = w * rows[:, 0].astype(np.float64) * _lib.FX_SCALE
+            out.append(dict(structure=s, ehss_angstrom2=summarize(ehss),
+                            ehss_tail_bound_mean_angstrom2=float(np.mean(2 * w * rows[:, 2].astype(np.float64))),
+                            ehss_unresolved_rays_total=int(rows[:, 2].sum())))
+        return out

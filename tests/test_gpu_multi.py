@@ -62,8 +62,12 @@ def test_structure_shards_add_up_to_one_batch(eb):
     full.upload()
     full.build()
     full.trace()
-    ref = full.scatter().clone()
+    ref = full.exchange().clone()
     np.testing.assert_array_equal(ref.cpu().numpy(), full.batch.plan.packed.cpu().numpy())
+    # the merged integers read out as BatchCCS reads its own
+    for a, b in zip(full.summaries(), full.batch.download()):
+        assert a['ehss_angstrom2'] == b['ehss_angstrom2']
+        assert a['ehss_unresolved_rays_total'] == b['ehss_unresolved_rays_total']
     total = torch.zeros_like(ref)
     owners = []
     for rank in range(3):

@@ -342,3 +342,27 @@ def test_structure_shards_exchange_with_two_gloo_ranks():
     assert mines == list(range(len(sizes)))
     for rank, mine, packed in got:
         assert packed == ref, rank
+
+
+def test_sharded_summaries_read_the_merged_integers():
+    """summaries() turns the merged block integers into per-structure CCS
+    with the blocks' impact-disk weights (pi R^2 / rays, fixed point 2^-36)."""
+    from ehss_b200 import blocks, _lib
+    from ehss_b200.batch import enclosing_radius
+    rng = np.random.default_rng(9)
+    structures = [(rng.normal(size=(n, 3)), np.full(n, 1.5)) for n in (12, 40)]
+    saved = blocks._RESULT_WORDS
+    blocks._RESULT_WORDS = _FakeBatch.W
+    try:
+        job = D.ShardedBatch(structures, [14, 15], [1, 2], 0, 1, repeats=3, cap=8, batch_factory=_FakeBatch)
+        job.step()
+        summ = job.summaries()
+    finally:
+        blocks._RESULT_WORDS = saved
+    res = job.batch.packed_np[:2 * 3 * _FakeBatch.W].reshape(6, _FakeBatch.W)
+    for s, lg in enumerate((14, 15)):
+        R = enclosing_radius(*structures[s])
+        w = np.pi * R * R / 2 ** lg
+        vals = w * res[3 * s:3 * s + 3, 0].astype(np.float64) * _lib.FX_SCALE
+        assert summ[s]['ehss_angstrom2']['mean'] == pytest.approx(vals.mean(), rel=1e-15)
+        assert summ[s]['ehss_unresolved_rays_total'] == int(res[3 * s:3 * s + 3, 2].sum())
