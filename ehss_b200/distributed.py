@@ -197,7 +197,7 @@ class ShardedBatch:
             radius = enclosing_radius(c, r)
             w = np.pi * radius * radius / float(1 << lg)
             rows = res[s * R:(s + 1) * R]
-            ehss = w * rows[:, 0].astype(np.float64) * _lib.FX_SCALE
+            ehss = w * (rows[:, 0].astype(np.float64) * _lib.FX_SCALE)
             out.append(dict(structure=s, ehss_angstrom2=summarize(ehss),
                             ehss_tail_bound_mean_angstrom2=float(np.mean(2 * w * rows[:, 2].astype(np.float64))),
                             ehss_unresolved_rays_total=int(rows[:, 2].sum())))

@@ -363,6 +363,6 @@ def test_sharded_summaries_read_the_merged_integers():
     for s, lg in enumerate((14, 15)):
         R = enclosing_radius(*structures[s])
         w = np.pi * R * R / 2 ** lg
-        vals = w * res[3 * s:3 * s + 3, 0].astype(np.float64) * _lib.FX_SCALE
+        vals = w * (res[3 * s:3 * s + 3, 0].astype(np.float64) * _lib.FX_SCALE)
         assert summ[s]['ehss_angstrom2']['mean'] == pytest.approx(vals.mean(), rel=1e-15)
         assert summ[s]['ehss_unresolved_rays_total'] == int(res[3 * s:3 * s + 3, 2].sum())
