@@ -491,6 +491,20 @@ struct LaneRay {
     double o[3], d[3], din[3];
 };
 
+// The fused kernel's dynamic shared memory: per-warp accumulators, per-lane
+// FP64 ray state, then the lanes' traversal-stack columns (and, for ray
+// blocks, the lanes' ray weights).
+extern __shared__ __align__(16) unsigned char smem_raw[];
+
+// Byte offset of the stack columns.  Recomputed from blockDim wherever a
+// stack entry is addressed, so no lane keeps a pointer to its column in
+// registers (the fused kernel runs at its 64-register bound: holding the
+// pointer and the column stride cost 24 bytes of spills per thread and 1.8 %
+// of trace time on the mixed 256-globule batch).
+__device__ __forceinline__ unsigned stack_off() {
+    return (unsigned)(sizeof(WarpAcc) * (blockDim.x >> 5) + sizeof(LaneRay) * blockDim.x);
+}
+
 __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long x) {
     for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
     return x;
@@ -529,14 +543,16 @@ struct Walker {
     double best;
     int best_rank, best_id;
     unsigned box, sphere;
-    int2* sstack;          // this lane's shared-memory stack column
-    int stride;            // entries are stride apart (blockDim.x)
     int sdepth;            // entries kept in shared memory (launch parameter)
+    // shared-memory stack entry i of this lane
+    __device__ __forceinline__ int2* slot(int i) const {
+        return reinterpret_cast<int2*>(smem_raw + stack_off()) + i * blockDim.x + threadIdx.x;
+    }
     int deep_ref[kStackDepth];
     float deep_t[kStackDepth];
 
     __device__ __forceinline__ void push(int ref, float t) {
-        if (sp < sdepth) sstack[sp * stride] = make_int2(ref, __float_as_int(t));
+        if (sp < sdepth) *slot(sp) = make_int2(ref, __float_as_int(t));
         else if (sp < kStackDepth) { deep_ref[sp - sdepth] = ref; deep_t[sp - sdepth] = t; }
         else { error = true; return; }
         ++sp;
@@ -555,7 +571,7 @@ struct Walker {
             --sp;
             int ref;
             float t;
-            if (sp < sdepth) { int2 e = sstack[sp * stride]; ref = e.x; t = __int_as_float(e.y); }
+            if (sp < sdepth) { int2 e = *slot(sp); ref = e.x; t = __int_as_float(e.y); }
             else { ref = deep_ref[sp - sdepth]; t = deep_t[sp - sdepth]; }
             if (t <= U) return ref;
         }
@@ -686,7 +702,6 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                                                    uint64_t* hist, uint64_t* ledger, unsigned long long* work,
                                                    int n_parts, int smem_stack, ehss_residual* residual,
                                                    long long residual_capacity, unsigned long long* residual_count) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     WarpAcc& A = reinterpret_cast<WarpAcc*>(smem_raw)[warp];
     LaneRay& L = reinterpret_cast<LaneRay*>(smem_raw + sizeof(WarpAcc) * nwarps)[threadIdx.x];
@@ -695,8 +710,6 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
     double* rho_lane = reinterpret_cast<double*>(stack_base + smem_stack * blockDim.x) + threadIdx.x;
     const unsigned lt_mask = (1u << lane) - 1u;
     Walker<EXACT, COUNT> W;
-    W.sstack = stack_base + threadIdx.x;
-    W.stride = blockDim.x;
     W.sdepth = smem_stack;
     int scan = 0;
     while (true) {
