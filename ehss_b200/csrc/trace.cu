@@ -543,7 +543,6 @@ struct Walker {
     double best;
     int best_rank, best_id;
     unsigned box, sphere;
-    int sdepth;            // entries kept in shared memory (launch parameter)
     // shared-memory stack entry i of this lane
     __device__ __forceinline__ int2* slot(int i) const {
         return reinterpret_cast<int2*>(smem_raw + stack_off()) + i * blockDim.x + threadIdx.x;
@@ -551,7 +550,7 @@ struct Walker {
     int deep_ref[kStackDepth];
     float deep_t[kStackDepth];
 
-    __device__ __forceinline__ void push(int ref, float t) {
+    __device__ __forceinline__ void push(int ref, float t, int sdepth) {
         if (sp < sdepth) *slot(sp) = make_int2(ref, __float_as_int(t));
         else if (sp < kStackDepth) { deep_ref[sp - sdepth] = ref; deep_t[sp - sdepth] = t; }
         else { error = true; return; }
@@ -566,7 +565,7 @@ struct Walker {
         overflow = grazing = error = false;
         if (EXACT) { best = CUDART_INF; best_rank = -1; best_id = -1; }
     }
-    __device__ __forceinline__ int pop() {
+    __device__ __forceinline__ int pop(int sdepth) {
         while (sp > 0) {
             --sp;
             int ref;
@@ -577,13 +576,13 @@ struct Walker {
         }
         return kSentinel;
     }
-    __device__ __forceinline__ int visit(const float4* nodes, int node) {
+    __device__ __forceinline__ int visit(const float4* nodes, int node, int sdepth) {
         Hits4 h = visit4(nodes, node, r, U);
         if (COUNT) box += 4;
-        if (h.n == 0) return pop();
-        if (h.n > 3) push(h.ref[3], h.t[3]);
-        if (h.n > 2) push(h.ref[2], h.t[2]);
-        if (h.n > 1) push(h.ref[1], h.t[1]);
+        if (h.n == 0) return pop(sdepth);
+        if (h.n > 3) push(h.ref[3], h.t[3], sdepth);
+        if (h.n > 2) push(h.ref[2], h.t[2], sdepth);
+        if (h.n > 1) push(h.ref[1], h.t[1], sdepth);
         return h.ref[0];
     }
     __device__ __forceinline__ void add_candidate(int k, float lo) {
@@ -710,7 +709,6 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
     double* rho_lane = reinterpret_cast<double*>(stack_base + smem_stack * blockDim.x) + threadIdx.x;
     const unsigned lt_mask = (1u << lane) - 1u;
     Walker<EXACT, COUNT> W;
-    W.sdepth = smem_stack;
     int scan = 0;
     while (true) {
         long long c = 0;
@@ -868,10 +866,10 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                     // inner nodes; the first leaf reached is postponed
                     while (W.cur >= 0 && W.cur != kSentinel) {
                         if (W.cur >= n_nodes || ++W.steps > 2 * n_nodes + 2) { W.error = true; W.cur = kSentinel; break; }
-                        W.cur = W.visit(S.nodes, W.cur);
+                        W.cur = W.visit(S.nodes, W.cur, smem_stack);
                         if (W.cur < 0 && W.leaf == kNoLeaf) {
                             W.leaf = W.cur;
-                            W.cur = W.pop();
+                            W.cur = W.pop(smem_stack);
                         }
                         if (!__any_sync(__activemask(), W.leaf == kNoLeaf)) break;
                     }
@@ -881,7 +879,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                         W.leaf = kNoLeaf;
                         if (W.cur < 0) {
                             W.leaf = W.cur;
-                            W.cur = W.pop();
+                            W.cur = W.pop(smem_stack);
                         }
                     }
                     if (W.cur == kSentinel) status = kDone;
