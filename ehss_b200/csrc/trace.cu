@@ -725,15 +725,12 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
         const ehss_block* B = blocks + bi;
         if ((B->precision == EHSS_PREC_FP64) != EXACT) continue;     // the other instantiation's chunk
         if (((B->flags & EHSS_BLOCK_RAYS) != 0) != RAYS) continue;
-        const int cap = B->cap;
-        const uint32_t flags = B->flags;
         const int64_t ray0 = (c - B->chunk_begin) * (int64_t)chunk_rays;
         const int cnt = (int)min((long long)chunk_rays, (long long)((1ll << B->log2_rays) - ray0));
         // only the scene's base stays live across the phases; each phase rebuilds the view
         // it needs from the (L1-resident) header, which keeps the traversal's registers free
         const void* const sbase = B->scene;
         const bool ok = scene_view(sbase).h->magic == kSceneMagic && scene_view(sbase).h->status == 0;
-        const int n_nodes = scene_view(sbase).h->n_nodes;
         if (lane < kSmemBins) { A.count[lane] = 0; A.ledger[lane] = 0; }
         if (lane == 0) {
             const uint4 b0 = make_uint4(B->base[0], B->base[1], B->base[2], B->base[3]);
@@ -773,7 +770,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                         atomicAdd(&A.fp64, f);
                     }
                 }
-                if (k < 0 || bounces >= cap) {
+                if (k < 0 || bounces >= __ldg(&B->cap)) {
                     bool escaped = k < 0;
                     unsigned long long fx = 0;
                     if (escaped) {
@@ -834,7 +831,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
 #pragma unroll
                             for (int i = 0; i < 3; ++i) { L.o[i] = ray.o[i]; L.d[i] = ray.d[i]; L.din[i] = ray.d[i]; }
                         }
-                        if (flags & EHSS_BLOCK_PA) {
+                        if (__ldg(&B->flags) & EHSS_BLOCK_PA) {
                             LocalStats pst;
                             if (anyhit(S, L.o, L.d, -1, pst)) {
                                 atomicAdd(&A.pa, 1u);
@@ -845,7 +842,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                         }
                         bounces = 0;
                         last_rank = -1;
-                        if (flags & EHSS_BLOCK_EHSS) {
+                        if (__ldg(&B->flags) & EHSS_BLOCK_EHSS) {
                             W.reset();
                             if (!setup_ray(S.h, L.o, L.d, W.r)) W.error = true;
                             atomicAdd(&A.queries, 1u);
@@ -865,6 +862,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                 if (status == kTraverse) {
                     // inner nodes; the first leaf reached is postponed
                     while (W.cur >= 0 && W.cur != kSentinel) {
+                        const int n_nodes = __ldg(&S.h->n_nodes);
                         if (W.cur >= n_nodes || ++W.steps > 2 * n_nodes + 2) { W.error = true; W.cur = kSentinel; break; }
                         W.cur = W.visit(S.nodes, W.cur, smem_stack);
                         if (W.cur < 0 && W.leaf == kNoLeaf) {
@@ -911,7 +909,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
             for (int i = 0; i < 7; ++i)
                 if (v[i]) atomicAdd((unsigned long long*)&R->stats[slot[i]], v[i]);
         }
-        if (lane < kSmemBins && lane <= cap) {
+        if (lane < kSmemBins && lane <= B->cap) {
             if (A.count[lane])
                 atomicAdd((unsigned long long*)&hist[B->hist_offset + lane], (unsigned long long)A.count[lane]);
             if (A.ledger[lane]) atomicAdd((unsigned long long*)&ledger[B->hist_offset + lane], A.ledger[lane]);
