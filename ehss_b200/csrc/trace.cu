@@ -49,7 +49,7 @@ struct LocalStats {
 };
 
 struct RayF {
-    float ox, oy, oz, dx, dy, dz, ix, iy, iz, oix, oiy, oiz, Ep, Edisc;
+    float ox, oy, oz, dx, dy, dz, ix, iy, iz, Ep, Edisc;
 };
 
 __device__ __forceinline__ float safe_rcp(float x) {
@@ -68,7 +68,6 @@ __device__ __forceinline__ bool setup_ray(const SceneHeader* H, const double* o,
     float a = sqrtf(fmaf(r.ox, r.ox, fmaf(r.oy, r.oy, r.oz * r.oz)));
     if (!(a <= 3.0f * S)) return false;
     r.ix = safe_rcp(r.dx); r.iy = safe_rcp(r.dy); r.iz = safe_rcp(r.dz);
-    r.oix = r.ox * r.ix; r.oiy = r.oy * r.iy; r.oiz = r.oz * r.iz;
     float A = a + S;
     r.Ep = A * (32.0f * kU32);
     float rm = H->rmax_f;
@@ -77,11 +76,13 @@ __device__ __forceinline__ bool setup_ray(const SceneHeader* H, const double* o,
 }
 
 // Slab test of one child box against [0, U]; returns entry distance or +inf.
-__device__ __forceinline__ float box_enter(const RayF& r, float lx, float hx, float ly, float hy, float lz, float hz,
-                                           float U) {
-    float tlx = fmaf(lx, r.ix, -r.oix), thx = fmaf(hx, r.ix, -r.oix);
-    float tly = fmaf(ly, r.iy, -r.oiy), thy = fmaf(hy, r.iy, -r.oiy);
-    float tlz = fmaf(lz, r.iz, -r.oiz), thz = fmaf(hz, r.iz, -r.oiz);
+// oi = o * inv per axis, formed once per node visit (held per lane it would
+// cost three registers of the fused kernel).
+__device__ __forceinline__ float box_enter(const RayF& r, float oix, float oiy, float oiz, float lx, float hx, float ly,
+                                           float hy, float lz, float hz, float U) {
+    float tlx = fmaf(lx, r.ix, -oix), thx = fmaf(hx, r.ix, -oix);
+    float tly = fmaf(ly, r.iy, -oiy), thy = fmaf(hy, r.iy, -oiy);
+    float tlz = fmaf(lz, r.iz, -oiz), thz = fmaf(hz, r.iz, -oiz);
     float tmin = fmaxf(fmaxf(fminf(tlx, thx), fminf(tly, thy)), fmaxf(fminf(tlz, thz), 0.0f));
     float tmax = fminf(fminf(fmaxf(tlx, thx), fmaxf(tly, thy)), fminf(fmaxf(tlz, thz), U));
     return tmin <= tmax ? tmin : CUDART_INF_F;
@@ -109,10 +110,11 @@ __device__ __forceinline__ Hits4 visit4(const float4* nodes, int node, const Ray
     Hits4 h;
     h.ref[0] = __float_as_int(rf.x); h.ref[1] = __float_as_int(rf.y);
     h.ref[2] = __float_as_int(rf.z); h.ref[3] = __float_as_int(rf.w);
-    h.t[0] = box_enter(r, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, U);
-    h.t[1] = box_enter(r, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, U);
-    h.t[2] = box_enter(r, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, U);
-    h.t[3] = box_enter(r, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, U);
+    const float oix = r.ox * r.ix, oiy = r.oy * r.iy, oiz = r.oz * r.iz;
+    h.t[0] = box_enter(r, oix, oiy, oiz, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, U);
+    h.t[1] = box_enter(r, oix, oiy, oiz, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, U);
+    h.t[2] = box_enter(r, oix, oiy, oiz, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, U);
+    h.t[3] = box_enter(r, oix, oiy, oiz, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, U);
 #pragma unroll
     for (int c = 0; c < 4; ++c)
         if (h.ref[c] == kEmptyChild) h.t[c] = CUDART_INF_F;
