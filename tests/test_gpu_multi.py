@@ -49,6 +49,11 @@ def test_ray_windows_add_up_to_one_launch(eb):
         plan.packed.copy_(total)
         a, b = plan.collect(), whole.collect()
         assert [x['ehss_angstrom2'] for x in a] == [x['ehss_angstrom2'] for x in b]
+    # an empty window (more ranks than work at the end of a list) traces nothing and leaves zeros
+    plan = BlockPlan(jobs)
+    plan.window = (7, 7)
+    plan.enqueue()
+    assert int(plan.packed.abs().sum()) == 0
 
 
 def test_structure_shards_add_up_to_one_batch(eb):
