@@ -24,6 +24,7 @@ from __future__ import annotations
 import math
 import time
 from dataclasses import dataclass, field
+from pathlib import Path
 
 import numpy as np
 
@@ -37,6 +38,20 @@ class CCSRequest:
     radii: np.ndarray
     seed: int = 190003
     arrival: float = 0.0            # seconds on the server clock
+
+    @classmethod
+    def from_xyz(cls, rid, path, frame=1, probe_radius=1.4, units='angstrom', exclude_hydrogen=False,
+                 radii_json=None, seed=190003, arrival=0.0):
+        """A request for one frame of an XYZ file, read and prepared as the
+        command line does (same dialect, radii table, probe radius, units and
+        recentring; the same ValueError messages for bad input)."""
+        from .ccs_cli import prepare_frame, radius_table, read_xyz
+        frames = read_xyz(path)
+        if not 1 <= int(frame) <= len(frames):
+            raise ValueError(f"{Path(path).name}: --frame {frame} exceeds {len(frames)} frames")
+        spheres, _ = prepare_frame(frames[int(frame) - 1], radius_table(radii_json), probe_radius, units,
+                                   exclude_hydrogen)
+        return cls(rid, spheres.centers, spheres.radii, seed=seed, arrival=arrival)
 
 
 @dataclass

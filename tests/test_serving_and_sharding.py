@@ -366,3 +366,21 @@ def test_sharded_summaries_read_the_merged_integers():
         vals = w * (res[3 * s:3 * s + 3, 0].astype(np.float64) * _lib.FX_SCALE)
         assert summ[s]['ehss_angstrom2']['mean'] == pytest.approx(vals.mean(), rel=1e-15)
         assert summ[s]['ehss_unresolved_rays_total'] == int(res[3 * s:3 * s + 3, 2].sum())
+
+
+def test_requests_from_xyz_files(tmp_path):
+    """XYZ jobs are read and prepared as the command line does and served."""
+    from ehss_b200 import ccs_cli
+    xyz = tmp_path / 'water.xyz'
+    xyz.write_text('3\nwater\nO 0 0 0\nH 0.9572 0 0\nH -0.239987 0.926627 0\n'
+                   '3\nsecond\nO 0 0 0\nH 0.96 0 0\nH -0.24 0.93 0\n')
+    req = CCSRequest.from_xyz('w2', xyz, frame=2, seed=5)
+    spheres, _ = ccs_cli.prepare_frame(ccs_cli.read_xyz(xyz)[1], ccs_cli.radius_table(None), 1.4)
+    np.testing.assert_array_equal(req.centers, spheres.centers)
+    np.testing.assert_array_equal(req.radii, spheres.radii)
+    assert req.seed == 5
+    with pytest.raises(ValueError, match='exceeds 2 frames'):
+        CCSRequest.from_xyz('w3', xyz, frame=3)
+    server = CCSServer(FakeExecutor(), target=0.01)
+    server.submit(req)
+    assert server.run()['w2']['converged']
