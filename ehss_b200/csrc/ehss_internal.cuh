@@ -25,7 +25,7 @@ namespace ehss {
 //   f[0] = lo.x[c]  f[1] = hi.x[c]  f[2] = lo.y[c]  f[3] = hi.y[c]
 //   f[4] = lo.z[c]  f[5] = hi.z[c]  f[6] = child ref[c] (int bits)  f[7] = unused
 // child >= 0: node index; child < 0: leaf ~(first << kLeafBits | (count - 1));
-// kEmptyChild marks an unused slot.  Node i is built from binary LBVH node i
+// kEmptyChild marks an unused slot, whose box is empty: lo = +inf, hi = -inf.  Node i is built from binary LBVH node i
 // with its grandchildren as children (children that are leaves, or subtrees
 // of at most leaf_size atoms, stay single slots), so only binary nodes at
 // even depth are ever referenced.

@@ -506,8 +506,9 @@ __device__ __forceinline__ void write_node4(float4* nodes, int64_t i, const floa
     for (int c = 0; c < 4; ++c) {
         bool used = c < n;
         for (int k = 0; k < 3; ++k) {
-            v[2 * k][c] = used ? __fsub_rd(box[c][k], eps) : 0.f;          // lo, rounded outward
-            v[2 * k + 1][c] = used ? __fadd_ru(box[c][3 + k], eps) : 0.f;  // hi
+            // lo and hi rounded outward; an unused slot's box is empty (lo = +inf, hi = -inf)
+            v[2 * k][c] = used ? __fsub_rd(box[c][k], eps) : CUDART_INF_F;
+            v[2 * k + 1][c] = used ? __fadd_ru(box[c][3 + k], eps) : -CUDART_INF_F;
         }
         r[c] = used ? ref[c] : kEmptyChild;
     }

@@ -75,16 +75,33 @@ __device__ __forceinline__ bool setup_ray(const SceneHeader* H, const double* o,
     return true;
 }
 
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 // Slab test of one child box against [0, U]; returns entry distance or +inf.
-// oi = o * inv per axis, formed once per node visit (held per lane it would
-// cost three registers of the fused kernel).
-__device__ __forceinline__ float box_enter(const RayF& r, float oix, float oiy, float oiz, float lx, float hx, float ly,
-                                           float hy, float lz, float hz, float U) {
-    float tlx = fmaf(lx, r.ix, -oix), thx = fmaf(hx, r.ix, -oix);
-    float tly = fmaf(ly, r.iy, -oiy), thy = fmaf(hy, r.iy, -oiy);
-    float tlz = fmaf(lz, r.iz, -oiz), thz = fmaf(hz, r.iz, -oiz);
-    float tmin = fmaxf(fmaxf(fminf(tlx, thx), fminf(tly, thy)), fmaxf(fminf(tlz, thz), 0.0f));
-    float tmax = fminf(fminf(fmaxf(tlx, thx), fmaxf(tly, thy)), fminf(fmaxf(tlz, thz), U));
+// The planes come as near (n*) and far (f*) per axis: with inv >= 0 the low
+// plane is met first, and fma(lo, inv, -oi) <= fma(hi, inv, -oi) because
+// rounding is monotone, so the near plane's distance is the slab minimum the
+// textbook test forms with fminf, bit for bit.  An unused slot holds the box
+// lo = +inf, hi = -inf, whose near distance is +inf on every axis, so it
+// misses without a check of its reference.  oi = o * inv per axis, formed
+// once per node visit (held per lane it would cost three registers of the
+// fused kernel).
+__device__ __forceinline__ float box_enter(const RayF& r, float oix, float oiy, float oiz, float nx, float fx, float ny,
+                                           float fy, float nz, float fz, float U) {
+    float tnx = fmaf(nx, r.ix, -oix), tfx = fmaf(fx, r.ix, -oix);
+    float tny = fmaf(ny, r.iy, -oiy), tfy = fmaf(fy, r.iy, -oiy);
+    float tnz = fmaf(nz, r.iz, -oiz), tfz = fmaf(fz, r.iz, -oiz);
+    float tmin = max3f(tnx, tny, fmaxf(tnz, 0.0f));
+    float tmax = min3f(tfx, tfy, fminf(tfz, U));
     return tmin <= tmax ? tmin : CUDART_INF_F;
 }
 
@@ -105,19 +122,18 @@ __device__ __forceinline__ void cswap(Hits4& h, int a, int b) {
 
 __device__ __forceinline__ Hits4 visit4(const float4* nodes, int node, const RayF& r, float U) {
     const float4* nd = nodes + 8 * (int64_t)node;
-    float4 lx = __ldg(nd), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
-    float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5), rf = __ldg(nd + 6);
+    // near and far plane rows by the direction's sign per axis (the node stores lo, hi)
+    const int sx = __float_as_uint(r.ix) >> 31, sy = __float_as_uint(r.iy) >> 31, sz = __float_as_uint(r.iz) >> 31;
+    float4 nx = __ldg(nd + sx), fx = __ldg(nd + (1 - sx)), ny = __ldg(nd + (2 + sy)), fy = __ldg(nd + (3 - sy));
+    float4 nz = __ldg(nd + (4 + sz)), fz = __ldg(nd + (5 - sz)), rf = __ldg(nd + 6);
     Hits4 h;
     h.ref[0] = __float_as_int(rf.x); h.ref[1] = __float_as_int(rf.y);
     h.ref[2] = __float_as_int(rf.z); h.ref[3] = __float_as_int(rf.w);
     const float oix = r.ox * r.ix, oiy = r.oy * r.iy, oiz = r.oz * r.iz;
-    h.t[0] = box_enter(r, oix, oiy, oiz, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, U);
-    h.t[1] = box_enter(r, oix, oiy, oiz, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, U);
-    h.t[2] = box_enter(r, oix, oiy, oiz, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, U);
-    h.t[3] = box_enter(r, oix, oiy, oiz, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, U);
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-        if (h.ref[c] == kEmptyChild) h.t[c] = CUDART_INF_F;
+    h.t[0] = box_enter(r, oix, oiy, oiz, nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, U);
+    h.t[1] = box_enter(r, oix, oiy, oiz, nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, U);
+    h.t[2] = box_enter(r, oix, oiy, oiz, nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, U);
+    h.t[3] = box_enter(r, oix, oiy, oiz, nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, U);
     cswap(h, 0, 1); cswap(h, 2, 3); cswap(h, 0, 2); cswap(h, 1, 3); cswap(h, 1, 2);
     h.n = (h.t[0] != CUDART_INF_F) + (h.t[1] != CUDART_INF_F) + (h.t[2] != CUDART_INF_F) + (h.t[3] != CUDART_INF_F);
     return h;
