@@ -618,8 +618,12 @@ struct Walker {
         int first = code >> kLeafBits, cnt = (code & (kMaxLeaf - 1)) + 1;
         if (first + cnt > S.h->n_atoms) { error = true; return; }
         for (int k = first; k < first + cnt; ++k) {
-            if (k == last_rank) continue;
-            if (COUNT) ++sphere;
+            // FILTER: the start atom is excluded after the cheap reject below, which a ray
+            // leaving that atom's surface (moving away from its centre) nearly always takes
+            if (EXACT || COUNT) {
+                if (k == last_rank) continue;
+                if (COUNT) ++sphere;
+            }
             if (EXACT) {
                 double4 a = S.atoms64[k];
                 double t = entry64(L.o[0], L.o[1], L.o[2], L.d[0], L.d[1], L.d[2], a.x, a.y, a.z, a.w);
@@ -636,6 +640,7 @@ struct Walker {
                 float q = fmaf(px, px, fmaf(py, py, pz * pz));
                 float disc = fmaf(a.w, a.w, -q);
                 if (disc < -r.Edisc || b < -r.Ep) continue;
+                if (!COUNT && k == last_rank) continue;
                 float s = sqrtf(fmaxf(disc, 0.0f));
                 float t = b - s;
                 if (disc >= 2.0f * r.Edisc) {
