@@ -597,10 +597,11 @@ struct Walker {
     __device__ __forceinline__ int visit(const float4* nodes, int node, int sdepth) {
         Hits4 h = visit4(nodes, node, r, U);
         if (COUNT) box += 4;
-        if (h.n == 0) return pop(sdepth);
-        if (h.n > 3) push(h.ref[3], h.t[3], sdepth);
-        if (h.n > 2) push(h.ref[2], h.t[2], sdepth);
-        if (h.n > 1) push(h.ref[1], h.t[1], sdepth);
+        // the distances are sorted with misses at +inf
+        if (h.t[0] == CUDART_INF_F) return pop(sdepth);
+        if (h.t[3] != CUDART_INF_F) push(h.ref[3], h.t[3], sdepth);
+        if (h.t[2] != CUDART_INF_F) push(h.ref[2], h.t[2], sdepth);
+        if (h.t[1] != CUDART_INF_F) push(h.ref[1], h.t[1], sdepth);
         return h.ref[0];
     }
     __device__ __forceinline__ void add_candidate(int k, float lo) {
