@@ -18,8 +18,9 @@
 //     reference's FP64 formula; U is the running best distance rounded up.
 //   FILTER (EHSS_PREC_FP32): spheres are tested in FP32 with the
 //     cancellation-free perpendicular-distance discriminant
-//     disc = r^2 - |v - (v.d) d|^2 and a per-ray error bound (Ep on
-//     projections, Edisc on the discriminant).  Certain misses are dropped;
+//     disc = r^2 - |v - (v.d) d|^2 (the fused kernel: the shorter
+//     b^2 + (r^2 - |v|^2) under a widened bound) and a per-ray error bound
+//     (Ep on projections, Edisc on the discriminant).  Certain misses are dropped;
 //     certain hits give an interval [t - Et, t + Et] and lower U to t + Et;
 //     every sphere whose lower bound is <= U (certain or near-tangent) is
 //     kept in a 2-entry candidate list, re-tested in FP64 at the end with the
@@ -58,8 +59,11 @@ __device__ __forceinline__ float safe_rcp(float x) {
 }
 
 // FP32 copy of an FP64 ray in the scene frame; false when the origin is too
-// far from the centre for the FP32 error bounds (or not finite).
-__device__ __forceinline__ bool setup_ray(const SceneHeader* H, const double* o, const double* d, RayF& r) {
+// far from the centre for the FP32 error bounds (or not finite).  widen > 0
+// adds widen * (rmax^2 + A^2) to the discriminant bound, for the fused
+// kernel's shorter discriminant (kWidenShortDisc below).
+__device__ __forceinline__ bool setup_ray(const SceneHeader* H, const double* o, const double* d, RayF& r,
+                                          float widen = 0.0f) {
     r.ox = __double2float_rn(o[0] - H->center[0]);
     r.oy = __double2float_rn(o[1] - H->center[1]);
     r.oz = __double2float_rn(o[2] - H->center[2]);
@@ -72,8 +76,24 @@ __device__ __forceinline__ bool setup_ray(const SceneHeader* H, const double* o,
     r.Ep = A * (32.0f * kU32);
     float rm = H->rmax_f;
     r.Edisc = (8.0f * kU32) * rm * rm + 2.5f * rm * r.Ep + 8.0f * r.Ep * r.Ep;
+    if (widen > 0.0f) r.Edisc += widen * (rm * rm + A * A);
     return true;
 }
+
+// The fused kernel's FILTER leaf test forms disc = b^2 + (r^2 - |v|^2)
+// (two operations fewer, and a dependency chain three shorter, than
+// r^2 - |v - b d|^2; v = c - o, b = v.d, both computed as in the
+// cancellation-free form).  In exact arithmetic on the FP32 values the two
+// differ by 2 b db + b^2 (|d|^2 - 1), db the rounding of b (<= 3u |v|) and
+// | |d|^2 - 1 | <= 2.1u: at most 8.2u |v|^2.  Rounding r^2 - |v|^2 costs at
+// most 4u (|v|^2 + r^2) and the last fma u |disc|; the cancellation-free
+// value's own roundings, already inside Edisc, are at most 5.1u |v - b d|^2 +
+// u |disc| again, and where a classification depends on them (true disc >= 0,
+// or computed disc >= 2 Edisc) |v - b d|^2 <= rmax^2 + 2 Edisc.  With
+// |v| <= |o| + S <= A (1 + 4u) the difference stays below 12.3u A^2 + 11.1u
+// rmax^2, so adding 16u (rmax^2 + A^2) to Edisc keeps every certain miss,
+// certain-hit interval and grazing lower bound as sound as before (u = 2^-24).
+constexpr float kWidenShortDisc = 16.0f * kU32;
 
 __device__ __forceinline__ float max3f(float a, float b, float c) {
     float d;
@@ -637,9 +657,9 @@ struct Walker {
                 float4 a = __ldg(S.atoms + k);
                 float vx = a.x - r.ox, vy = a.y - r.oy, vz = a.z - r.oz;
                 float b = fmaf(vx, r.dx, fmaf(vy, r.dy, vz * r.dz));
-                float px = fmaf(-b, r.dx, vx), py = fmaf(-b, r.dy, vy), pz = fmaf(-b, r.dz, vz);
-                float q = fmaf(px, px, fmaf(py, py, pz * pz));
-                float disc = fmaf(a.w, a.w, -q);
+                // the short discriminant; r.Edisc is widened for it (kWidenShortDisc)
+                float w = fmaf(-vx, vx, fmaf(-vy, vy, fmaf(-vz, vz, a.w * a.w)));
+                float disc = fmaf(b, b, w);
                 if (disc < -r.Edisc || b < -r.Ep) continue;
                 if (!COUNT && k == last_rank) continue;
                 float s = sqrtf(fmaxf(disc, 0.0f));
@@ -826,7 +846,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                     ++bounces;
                     last_rank = k;
                     W.reset();
-                    if (!setup_ray(S.h, L.o, L.d, W.r)) W.error = true;   // bounce points lie within S
+                    if (!setup_ray(S.h, L.o, L.d, W.r, EXACT ? 0.0f : kWidenShortDisc)) W.error = true;   // bounce points lie within S
                     atomicAdd(&A.queries, 1u);
                     status = kTraverse;
                 }
@@ -868,7 +888,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                         last_rank = -1;
                         if (__ldg(&B->flags) & EHSS_BLOCK_EHSS) {
                             W.reset();
-                            if (!setup_ray(S.h, L.o, L.d, W.r)) W.error = true;
+                            if (!setup_ray(S.h, L.o, L.d, W.r, EXACT ? 0.0f : kWidenShortDisc)) W.error = true;
                             atomicAdd(&A.queries, 1u);
                             status = kTraverse;
                         }
