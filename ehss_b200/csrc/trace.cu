@@ -95,6 +95,22 @@ __device__ __forceinline__ bool setup_ray(const SceneHeader* H, const double* o,
 // certain-hit interval and grazing lower bound as sound as before (u = 2^-24).
 constexpr float kWidenShortDisc = 16.0f * kU32;
 
+// sqrt(disc) of a certain hit (computed disc >= 2 Edisc) and the error bound Et
+// of its entry and exit distances b -/+ sqrt(disc), from one reciprocal square
+// root: s = disc * y and Edisc / s = Edisc * y.  rsqrtf is within 2 ulp of 1/sqrt(disc) (the CUDA
+// math library's stated bound; at most 2.09 u measured over every float in
+// [2^-14, 2^8)), so s is within 5.01 u of sqrt(disc) and Edisc * y within
+// 5.01 u of Edisc / sqrt(disc).  With the roundings of s and of b -/+ s the
+// distance error stays below Ep + Edisc / sqrt(disc) + 6.01 u (|b| + s), which Et
+// covers with a factor-2 margin on its first two terms, as the correctly
+// rounded square root and quotient did before (u = 2^-24).
+__device__ __forceinline__ float certain_sqrt(float b, float disc, const RayF& r, float& Et) {
+    const float y = rsqrtf(disc);
+    const float s = disc * y;
+    Et = 2.0f * (r.Ep + r.Edisc * y) + 8.0f * kU32 * (fabsf(b) + s);
+    return s;
+}
+
 __device__ __forceinline__ float max3f(float a, float b, float c) {
     float d;
     asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
@@ -247,12 +263,11 @@ __device__ __noinline__ int nearest(const SceneView& S, const double* o, const d
                     float q = fmaf(px, px, fmaf(py, py, pz * pz));
                     float disc = fmaf(a.w, a.w, -q);
                     if (disc < -r.Edisc || b < -r.Ep) continue;          // certain miss
-                    float s = sqrtf(fmaxf(disc, 0.0f));
-                    float t = b - s;
                     float lo;
                     bool certain = false;
                     if (disc >= 2.0f * r.Edisc) {
-                        float Et = 2.0f * (r.Ep + __fdividef(r.Edisc, s)) + 4.0f * kU32 * (fabsf(b) + s);
+                        float Et;
+                        const float t = b - certain_sqrt(b, disc, r, Et);
                         if (t < -2.0f * Et) continue;                    // origin inside: no entry ahead
                         if (t > Et) {
                             certain = true;
@@ -355,10 +370,10 @@ __device__ __noinline__ bool anyhit(const SceneView& S, const double* o, const d
                 float q = fmaf(px, px, fmaf(py, py, pz * pz));
                 float disc = fmaf(a.w, a.w, -q);
                 if (disc < -r.Edisc) continue;
-                float s = sqrtf(fmaxf(disc, 0.0f));
-                float exitp = b + s;     // far root: the reference's -b + sqrt(disc) with b = x.d = -(v.d)
                 if (disc >= 2.0f * r.Edisc) {
-                    float Et = 2.0f * (r.Ep + __fdividef(r.Edisc, s)) + 4.0f * kU32 * (fabsf(b) + s);
+                    float Et;
+                    // far root: the reference's -b + sqrt(disc) with b = x.d = -(v.d)
+                    const float exitp = b + certain_sqrt(b, disc, r, Et);
                     if (exitp > Et) return true;
                     if (exitp < -2.0f * Et) continue;
                 } else if (b + sqrtf(fmaxf(disc, 0.0f) + r.Edisc) < -2.0f * r.Ep) {
@@ -662,10 +677,9 @@ struct Walker {
                 float disc = fmaf(b, b, w);
                 if (disc < -r.Edisc || b < -r.Ep) continue;
                 if (!COUNT && k == last_rank) continue;
-                float s = sqrtf(fmaxf(disc, 0.0f));
-                float t = b - s;
                 if (disc >= 2.0f * r.Edisc) {
-                    float Et = 2.0f * (r.Ep + __fdividef(r.Edisc, s)) + 4.0f * kU32 * (fabsf(b) + s);
+                    float Et;
+                    const float t = b - certain_sqrt(b, disc, r, Et);
                     if (t < -2.0f * Et) continue;
                     if (t > Et) {
                         float up = t + Et;
