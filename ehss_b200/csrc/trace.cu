@@ -929,8 +929,8 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                         }
                         if (!__any_sync(__activemask(), W.leaf == kNoLeaf)) break;
                     }
-                    // postponed leaf, then any leaf that comes next
-                    while (W.leaf != kNoLeaf) {
+                    // one leaf per lane and phase: a lane's next leaf joins the next phase
+                    if (W.leaf != kNoLeaf) {
                         W.leaf_tests(S, W.leaf, last_rank, L);
                         W.leaf = kNoLeaf;
                         if (W.cur < 0) {
@@ -938,7 +938,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                             W.cur = W.pop(smem_stack);
                         }
                     }
-                    if (W.cur == kSentinel) status = kDone;
+                    if (W.cur == kSentinel && W.leaf == kNoLeaf) status = kDone;
                 }
                 unsigned done = __ballot_sync(0xffffffffu, status == kDone);
                 unsigned trav = __ballot_sync(0xffffffffu, status == kTraverse);
