@@ -525,9 +525,11 @@ __global__ void k_source_rays(const void* scene, Sobol4Params p, int64_t first, 
 // One warp takes one chunk (chunk_rays consecutive positions of one block's
 // coherent Sobol enumeration) at a time.  Lanes are refilled with the chunk's
 // next ray as soon as theirs finishes.  Each warp alternates two phases:
-//   traverse  while-while walk (inner nodes, then postponed leaves) for every
-//             lane whose query is open, until at least `resolve_batch` lanes
-//             have finished their query or none is left traversing;
+//   traverse  while-while walk for every lane whose query is open: inner
+//             nodes until each lane holds a leaf (a lane holding one walks on
+//             to its next), then one leaf per lane, all lanes together;
+//             repeated until at least `resolve_batch` lanes have finished
+//             their query or none is left traversing;
 //   resolve   for all finished lanes together: FP64 candidate re-test,
 //             escape / cap / reflection, and new rays for finished rays.
 // Batching the FP64 work keeps most lanes of the warp busy in both phases.
@@ -925,7 +927,7 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
             const SceneView S = scene_view(sbase);
             while (true) {
                 if (status == kTraverse) {
-                    // inner nodes; the first leaf reached is postponed
+                    // inner nodes; the first leaf reached is held while the lane walks on
                     while (W.cur >= 0 && W.cur != kSentinel) {
                         const int n_nodes = __ldg(&S.h->n_nodes);
                         if (W.cur >= n_nodes || ++W.steps > 2 * n_nodes + 2) { W.error = true; W.cur = kSentinel; break; }
