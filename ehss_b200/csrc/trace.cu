@@ -524,14 +524,15 @@ __global__ void k_source_rays(const void* scene, Sobol4Params p, int64_t first, 
 //
 // One warp takes one chunk (chunk_rays consecutive positions of one block's
 // coherent Sobol enumeration) at a time.  Lanes are refilled with the chunk's
-// next ray as soon as theirs finishes.  Each warp alternates two phases:
+// next rays, kNewRayBatch or more at a time.  Each warp alternates two phases:
 //   traverse  while-while walk for every lane whose query is open: inner
 //             nodes until each lane holds a leaf (a lane holding one walks on
 //             to its next), then one leaf per lane, all lanes together;
 //             repeated until at least `resolve_batch` lanes have finished
-//             their query or none is left traversing;
+//             their query or wait for a new ray, or none is left traversing;
 //   resolve   for all finished lanes together: FP64 candidate re-test,
-//             escape / cap / reflection, and new rays for finished rays.
+//             escape / cap / reflection, and new rays once enough lanes
+//             wait for one.
 // Batching the FP64 work keeps most lanes of the warp busy in both phases.
 // The FP64 ray state (position, direction, incoming direction) waits in
 // shared memory while the lane traverses in FP32.
@@ -585,6 +586,10 @@ __device__ __forceinline__ uint4 block_point(const uint4* basis, uint4 base, uin
 }
 
 constexpr int kIdle = 0, kTraverse = 1, kDone = 2, kNeedRay = 3;
+// Lanes whose ray has finished wait for a new one until this many of a warp
+// do (16 of 32: the 256-globule batch traces in 23.9 ms against 24.6 with a
+// new ray at once, 24.2 with 8 and 24.2 with 24).
+constexpr int kNewRayBatch = 16;
 constexpr int kSentinel = INT32_MAX - 1;   // stack exhausted
 constexpr int kNoLeaf = INT32_MAX;
 
@@ -875,8 +880,10 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                 }
             }
             // ---- new rays for lanes whose ray finished ----
+            // made once kNewRayBatch lanes wait for one (or the chunk is used up, or no
+            // lane traverses), so that the FP64 impact-disk work runs at warp width
             unsigned need = __ballot_sync(0xffffffffu, status == kNeedRay);
-            if (need) {
+            if (need && (__popc(need) >= kNewRayBatch || pool >= cnt || !__any_sync(0xffffffffu, status == kTraverse))) {
                 const SceneView S = scene_view(sbase);
                 if (status == kNeedRay) {
                     int p = pool + __popc(need & lt_mask);
@@ -949,7 +956,8 @@ __global__ void __launch_bounds__(128, 8) k_blocks(const ehss_block* blocks, int
                     }
                     if (W.cur == kSentinel && W.leaf == kNoLeaf) status = kDone;
                 }
-                unsigned done = __ballot_sync(0xffffffffu, status == kDone);
+                // lanes waiting for a new ray count towards the resolve batch
+                unsigned done = __ballot_sync(0xffffffffu, status == kDone || status == kNeedRay);
                 unsigned trav = __ballot_sync(0xffffffffu, status == kTraverse);
                 if (!trav || __popc(done) >= resolve_batch) break;
             }
