@@ -22,7 +22,7 @@ from .blocks import DEFAULT_LAUNCH, BlockJob, BlockPlan
 from .device import torch
 
 SPACE = dict(block_threads=(64, 128), warps_per_sm=(16, 24, 32), chunk_rays=(128, 256, 512),
-             resolve_batch=(20, 28, 32), smem_stack=(4, 5, 8))
+             resolve_batch=(24, 30, 32), smem_stack=(4, 5, 8))
 
 
 def cache_path():

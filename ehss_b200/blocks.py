@@ -27,7 +27,7 @@ from .device import empty, ptr, stream_handle, torch
 _RESULT_WORDS = ct.sizeof(_lib.BlockResult) // 8
 _STATS0 = _lib.BlockResult.stats.offset // 8
 # chunk_rays 0: sized to the work (auto_chunk)
-DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=8, chunk_rays=0, resolve_batch=28, smem_stack=5,
+DEFAULT_LAUNCH = dict(block_threads=128, ctas_per_sm=8, chunk_rays=0, resolve_batch=30, smem_stack=5,
                       count_tests=False)
 
 
